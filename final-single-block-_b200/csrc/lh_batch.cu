@@ -1,0 +1,246 @@
+// Batched engine: many independent channel instances of uneven size advance
+// together.  Every substep issues the same kernels as a single instance, but
+// each launch's work table spans all live instances (instance, plane, block),
+// so a batch of N instances costs one launch per kernel class and chunk
+// round rather than N.  Each instance owns its device allocation; admission
+// is checked against an HBM budget.  One RK3 step of the current membership
+// is captured once in a CUDA graph and replayed until membership changes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "lh_engine.h"
+#include "lh_gpu.h"
+#include "lh_kernels.cuh"
+
+using namespace lh;
+
+struct lh_batch {
+    size_t budget = 0, used = 0;
+    std::vector<std::unique_ptr<DevInstance>> slots;  // nullptr = free slot
+    std::vector<int> live;                            // slot ids in launch order
+    Plan plan;
+    Inst *d_insts = nullptr;
+    size_t d_insts_cap = 0;
+    cudaStream_t st = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    bool dirty = true;
+    bool any_cfl = false;
+    std::string err;
+};
+
+static int bfail(lh_batch *b, int code, const std::string &m)
+{
+    if (b) b->err = m;
+    return code;
+}
+
+static int bcuda(lh_batch *b, cudaError_t e, const char *where)
+{
+    return bfail(b, e == cudaErrorMemoryAllocation ? LH_ENOMEM : LH_ECUDA,
+                 std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define BCK(call, where)                                        \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return bcuda(b, e_, where);      \
+    } while (0)
+
+static void drop_graph(lh_batch *b)
+{
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->gexec = nullptr;
+    b->graph = nullptr;
+}
+
+extern "C" int lh_batch_create(size_t budget, lh_batch **out)
+{
+    if (!out) return LH_EINVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return LH_ECUDA;
+    lh_batch *b = new (std::nothrow) lh_batch();
+    if (!b) return LH_ENOMEM;
+    b->budget = budget;
+    if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete b;
+        return LH_ECUDA;
+    }
+    *out = b;
+    return LH_OK;
+}
+
+extern "C" int lh_batch_destroy(lh_batch *b)
+{
+    if (!b) return LH_OK;
+    if (b->st) cudaStreamSynchronize(b->st);
+    drop_graph(b);
+    plan_free(b->plan);
+    if (b->d_insts) cudaFree(b->d_insts);
+    for (auto &s : b->slots)
+        if (s) instance_free(*s);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+    return LH_OK;
+}
+
+extern "C" const char *lh_batch_last_error(const lh_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+extern "C" size_t lh_instance_bytes(const lh_grid_desc *desc)
+{
+    if (!desc) return 0;
+    HostSetup hs;
+    if (!build_setup(*desc, hs).empty()) return 0;
+    Tiles t = default_tiles(hs.Mx, hs.Mz, hs.nxh, hs.nyu);
+    return instance_bytes(hs, t.chunk);
+}
+
+extern "C" int lh_batch_add(lh_batch *b, const lh_grid_desc *desc, const double *u1, const double *u2,
+                            const double *u3, const double *p, int *slot)
+{
+    if (!b || !desc || !u1 || !u2 || !u3 || !slot) return bfail(b, LH_EINVAL, "bad arguments");
+    auto d = std::unique_ptr<DevInstance>(new (std::nothrow) DevInstance());
+    if (!d) return bfail(b, LH_ENOMEM, "host allocation");
+    d->desc = *desc;
+    std::string why = build_setup(*desc, d->hs);
+    if (!why.empty()) return bfail(b, LH_EINVAL, why);
+    Tiles t = default_tiles(d->hs.Mx, d->hs.Mz, d->hs.nxh, d->hs.nyu);
+    const size_t need = instance_bytes(d->hs, t.chunk);
+    if (b->budget && b->used + need > b->budget)
+        return bfail(b, LH_ENOMEM, "HBM budget exhausted");
+    // instances are admitted between steps; wait for in-flight work first
+    BCK(cudaStreamSynchronize(b->st), "synchronize");
+    cudaError_t e = instance_alloc(*d, t.chunk, b->st);
+    if (e == cudaSuccess) e = instance_upload(*d, u1, u2, u3, p, b->st);
+    if (e != cudaSuccess) {
+        instance_free(*d);
+        return bcuda(b, e, "admit");
+    }
+    b->used += d->bytes;
+    int id = -1;
+    for (size_t k = 0; k < b->slots.size(); k++)
+        if (!b->slots[k]) {
+            id = (int)k;
+            break;
+        }
+    if (id < 0) {
+        id = (int)b->slots.size();
+        b->slots.emplace_back();
+    }
+    b->slots[id] = std::move(d);
+    b->dirty = true;
+    *slot = id;
+    return LH_OK;
+}
+
+extern "C" int lh_batch_remove(lh_batch *b, int slot)
+{
+    if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot]) return bfail(b, LH_EINVAL, "bad slot");
+    BCK(cudaStreamSynchronize(b->st), "synchronize");
+    b->used -= b->slots[slot]->bytes;
+    instance_free(*b->slots[slot]);
+    b->slots[slot].reset();
+    b->dirty = true;
+    return LH_OK;
+}
+
+static int rebuild(lh_batch *b)
+{
+    if (!b->dirty) return LH_OK;
+    drop_graph(b);
+    b->live.clear();
+    std::vector<const DevInstance *> v;
+    std::vector<Inst> hi;
+    b->any_cfl = false;
+    int maxMx = 0, maxMz = 0, maxnxh = 0, maxnyu = 0;
+    for (size_t k = 0; k < b->slots.size(); k++)
+        if (b->slots[k]) {
+            b->live.push_back((int)k);
+            v.push_back(b->slots[k].get());
+            hi.push_back(b->slots[k]->inst);
+            b->any_cfl |= b->slots[k]->desc.dt_mode == LH_DT_CFL;
+            maxMx = std::max(maxMx, b->slots[k]->hs.Mx);
+            maxMz = std::max(maxMz, b->slots[k]->hs.Mz);
+            maxnxh = std::max(maxnxh, b->slots[k]->hs.nxh);
+            maxnyu = std::max(maxnyu, b->slots[k]->hs.nyu);
+        }
+    if (v.empty()) {
+        b->dirty = false;
+        return LH_OK;
+    }
+    if (hi.size() > b->d_insts_cap) {
+        if (b->d_insts) cudaFree(b->d_insts);
+        b->d_insts = nullptr;
+        BCK(cudaMalloc(&b->d_insts, hi.size() * sizeof(Inst)), "alloc instance table");
+        b->d_insts_cap = hi.size();
+    }
+    BCK(cudaMemcpy(b->d_insts, hi.data(), hi.size() * sizeof(Inst), cudaMemcpyHostToDevice), "instance table");
+    Tiles t = default_tiles(maxMx, maxMz, maxnxh, maxnyu);
+    BCK(plan_build(b->plan, v, t), "plan");
+    BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal), "capture");
+    cudaError_t el = cudaSuccess;
+    for (int k = 1; k <= 3 && el == cudaSuccess; k++) el = launch_substep(b->plan, b->d_insts, k, b->any_cfl, b->st);
+    cudaGraph_t g = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(b->st, &g);
+    if (el != cudaSuccess) return bcuda(b, el, "capture launch");
+    if (ee != cudaSuccess) return bcuda(b, ee, "capture end");
+    b->graph = g;
+    BCK(cudaGraphInstantiate(&b->gexec, g, 0), "instantiate");
+    b->dirty = false;
+    return LH_OK;
+}
+
+extern "C" int lh_batch_step(lh_batch *b, int nsteps)
+{
+    if (!b || nsteps < 0) return bfail(b, LH_EINVAL, "bad arguments");
+    int rc = rebuild(b);
+    if (rc) return rc;
+    if (b->live.empty()) return LH_OK;
+    for (int s = 0; s < nsteps; s++) BCK(cudaGraphLaunch(b->gexec, b->st), "graph launch");
+    return LH_OK;
+}
+
+extern "C" int lh_batch_download(lh_batch *b, int slot, double *u1, double *u2, double *u3, double *p)
+{
+    if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot]) return bfail(b, LH_EINVAL, "bad slot");
+    BCK(instance_download(*b->slots[slot], u1, u2, u3, p, b->st), "download");
+    return LH_OK;
+}
+
+extern "C" int lh_batch_scalars(lh_batch *b, int slot, double *t, double *dt, int *iter)
+{
+    if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot]) return bfail(b, LH_EINVAL, "bad slot");
+    double sc[SC_COUNT];
+    int err = 0;
+    const Inst &I = b->slots[slot]->inst;
+    BCK(cudaMemcpyAsync(sc, I.sc, sizeof(sc), cudaMemcpyDeviceToHost, b->st), "scalars");
+    BCK(cudaMemcpyAsync(&err, I.err, sizeof(int), cudaMemcpyDeviceToHost, b->st), "scalars");
+    BCK(cudaStreamSynchronize(b->st), "scalars");
+    if (t) *t = sc[SC_T];
+    if (dt) *dt = sc[SC_DT];
+    if (iter) *iter = (int)sc[SC_ITER];
+    if (err & ERR_NONFINITE) return bfail(b, LH_EDEVICE, "instance state became non-finite");
+    return LH_OK;
+}
+
+extern "C" int lh_batch_count(const lh_batch *b)
+{
+    if (!b) return 0;
+    int n = 0;
+    for (auto &s : b->slots) n += s ? 1 : 0;
+    return n;
+}
+
+extern "C" int lh_batch_synchronize(lh_batch *b)
+{
+    if (!b) return LH_EINVAL;
+    BCK(cudaStreamSynchronize(b->st), "synchronize");
+    return LH_OK;
+}

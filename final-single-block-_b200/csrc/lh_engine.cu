@@ -1,0 +1,322 @@
+// Engine internals: device memory of an instance, the layout transforms at
+// the host boundary, work tables and the launch sequence of a substep.
+#include "lh_engine.h"
+
+#include <algorithm>
+#include <cstring>
+
+#include "lh_kernels.cuh"
+
+namespace lh {
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+Tiles default_tiles(int Mx, int Mz, int nxh, int nyu)
+{
+    Tiles t;
+    const size_t target = 48 * 1024;
+    t.bc_zinv = std::max(1, std::min(nxh, (int)(target / (32 * (size_t)Mz))));
+    t.br_x = std::max(1, std::min(Mz, (int)(target / (96 * (size_t)Mx))));
+    t.bc_zfwd = std::max(1, std::min(nxh, (int)(target / (192 * (size_t)Mz))));
+    t.threads = 256;
+    const size_t per_plane = (size_t)kNumProducts * Mz * nxh * sizeof(double2);
+    const size_t budget = 40ull << 20;  // staging kept well inside the 126 MB L2
+    t.chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nyu, budget / per_plane));
+    return t;
+}
+
+size_t smem_zinv(const Tiles &t, int Mz) { return 2 * (size_t)Mz * t.bc_zinv * sizeof(double2); }
+size_t smem_x(const Tiles &t, int Mx) { return 2 * (size_t)Mx * 3 * t.br_x * sizeof(double2); }
+size_t smem_zfwd(const Tiles &t, int Mz) { return 2 * (size_t)Mz * kNumProducts * t.bc_zfwd * sizeof(double2); }
+
+namespace {
+struct Carver {
+    size_t off = 0;
+    char *base = nullptr;
+    template <class T>
+    T *take(size_t n)
+    {
+        size_t o = off;
+        off = align256(off + n * sizeof(T));
+        return base ? reinterpret_cast<T *>(base + o) : nullptr;
+    }
+};
+
+// Lay out every buffer of an instance; with base == nullptr it only sizes.
+void carve(const HostSetup &s, int chunk, Carver &c, Inst &I, double2 **stage, size_t *stage_elems)
+{
+    const size_t nc = s.nc, nu = s.nyu + 2, nv = s.nyv + 2, np = s.nyu;
+    I.yu = c.take<double>(nu);
+    I.yv = c.take<double>(nv);
+    I.dthdyu = c.take<double>(nu);
+    I.dthdyv = c.take<double>(nv);
+    I.dyu2i = c.take<double>(3 * nu);
+    I.dyv2i = c.take<double>(3 * nv);
+    I.kx = c.take<double>(s.nxh);
+    I.kz = c.take<double>(s.Nz);
+    I.k2x = c.take<double>(s.nxh);
+    I.k2z = c.take<double>(s.Nz);
+    I.DG1 = c.take<double>(s.nyu + 1);
+    I.DG2 = c.take<double>(np * nc);
+    I.DG3 = c.take<double>(np * nc);
+    I.twz = c.take<double2>(s.Mz);
+    I.twx = c.take<double2>(s.Mx);
+    I.U1 = c.take<double2>(nu * nc);
+    I.U2 = c.take<double2>(nv * nc);
+    I.U3 = c.take<double2>(nu * nc);
+    I.P = c.take<double2>(np * nc);
+    I.NU1 = c.take<double2>(np * nc);
+    I.NU2 = c.take<double2>(np * nc);
+    I.NU3 = c.take<double2>(np * nc);
+    I.NXZ1 = c.take<double2>(np * nc);
+    I.NXZ2 = c.take<double2>(np * nc);
+    I.NXZ3 = c.take<double2>(np * nc);
+    I.UVF = c.take<double2>((np + 1) * nc);
+    I.WVF = c.take<double2>((np + 1) * nc);
+    I.VVC = c.take<double2>(nu * nc);
+    I.FACU = c.take<double>(nu * nc);
+    I.FACV = c.take<double>(nv * nc);
+    I.PSI = c.take<double2>(np * nc);
+    I.U11 = c.take<double>(nu);
+    I.F11 = c.take<double>(nu);
+    I.S = c.take<double2>((size_t)chunk * kNumProducts * s.Mz * s.nxh);
+    I.sc = c.take<double>(SC_COUNT);
+    I.err = c.take<int>(8);
+    *stage_elems = nu * nc;
+    *stage = c.take<double2>(*stage_elems);
+}
+}  // namespace
+
+size_t instance_bytes(const HostSetup &hs, int chunk)
+{
+    Carver c;
+    Inst I{};
+    double2 *st;
+    size_t se;
+    carve(hs, chunk, c, I, &st, &se);
+    return c.off;
+}
+
+cudaError_t instance_alloc(DevInstance &d, int chunk, cudaStream_t st)
+{
+    const HostSetup &s = d.hs;
+    Carver c;
+    Inst &I = d.inst;
+    memset(&I, 0, sizeof(I));
+    carve(s, chunk, c, I, &d.stage, &d.stage_elems);
+    d.bytes = c.off;
+    cudaError_t e = cudaMalloc(&d.block, d.bytes);
+    if (e != cudaSuccess) {
+        d.block = nullptr;
+        return e;
+    }
+    c = Carver();
+    c.base = (char *)d.block;
+    carve(s, chunk, c, I, &d.stage, &d.stage_elems);
+    e = cudaMemsetAsync(d.block, 0, d.bytes, st);
+    if (e != cudaSuccess) return e;
+    auto up = [&](const void *dst, const void *src, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMemcpyAsync(const_cast<void *>(dst), src, bytes, cudaMemcpyHostToDevice, st);
+    };
+    up(I.yu, s.yu.data(), s.yu.size() * 8);
+    up(I.yv, s.yv.data(), s.yv.size() * 8);
+    up(I.dthdyu, s.dthdyu.data(), s.dthdyu.size() * 8);
+    up(I.dthdyv, s.dthdyv.data(), s.dthdyv.size() * 8);
+    up(I.dyu2i, s.dyu2i.data(), s.dyu2i.size() * 8);
+    up(I.dyv2i, s.dyv2i.data(), s.dyv2i.size() * 8);
+    up(I.kx, s.kx.data(), s.kx.size() * 8);
+    up(I.kz, s.kz.data(), s.kz.size() * 8);
+    up(I.k2x, s.k2x.data(), s.k2x.size() * 8);
+    up(I.k2z, s.k2z.data(), s.k2z.size() * 8);
+    up(I.DG1, s.DG1.data(), s.DG1.size() * 8);
+    up(I.DG2, s.DG2.data(), s.DG2.size() * 8);
+    up(I.DG3, s.DG3.data(), s.DG3.size() * 8);
+    up(I.twz, s.twz.data(), s.twz.size() * 8);
+    up(I.twx, s.twx.data(), s.twx.size() * 8);
+    if (e != cudaSuccess) return e;
+    I.Nx = s.Nx;
+    I.Nz = s.Nz;
+    I.Mx = s.Mx;
+    I.Mz = s.Mz;
+    I.nxh = s.nxh;
+    I.nc = s.nc;
+    I.nyu = s.nyu;
+    I.nyv = s.nyv;
+    I.dt_mode = d.desc.dt_mode;
+    I.flag_ctpress = d.desc.flag_ctpress;
+    I.nradz = (int)s.radz.size();
+    I.nradx = (int)s.radx.size();
+    for (int k = 0; k < I.nradz; k++) I.radz[k] = s.radz[k];
+    for (int k = 0; k < I.nradx; k++) I.radx[k] = s.radx[k];
+    I.Re = d.desc.Re;
+    I.alp = d.desc.alp;
+    I.bet = d.desc.bet;
+    I.CFL = d.desc.CFL;
+    I.dtv = s.dtv;
+    I.dt_fixed = d.desc.dt;
+    I.gw1 = s.gw1;
+    I.gw2 = s.gw2;
+    I.gwbc = s.gwbc;
+    I.gwi1 = s.gwi1;
+    I.gwi2 = s.gwi2;
+    I.ddthetavi = s.ddthetavi;
+    I.chunk = chunk;
+    return cudaStreamSynchronize(st);
+}
+
+void instance_free(DevInstance &d)
+{
+    if (d.block) cudaFree(d.block);
+    d.block = nullptr;
+}
+
+static cudaError_t upload_field(DevInstance &d, const double *src, double2 *dst, int len, cudaStream_t st)
+{
+    const int nc = d.hs.nc;
+    if (!src) return cudaMemsetAsync(dst, 0, (size_t)len * nc * sizeof(double2), st);
+    cudaError_t e = cudaMemcpyAsync(d.stage, src, (size_t)len * nc * sizeof(double2), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    dim3 grid((nc + 31) / 32, (len + 31) / 32), block(32, 8);
+    k_col_to_plane<<<grid, block, 0, st>>>(d.stage, dst, len, nc);
+    return cudaGetLastError();
+}
+
+cudaError_t download_field(const DevInstance &d, const double2 *src, int len, double *dst, cudaStream_t st)
+{
+    const int nc = d.hs.nc;
+    dim3 grid((nc + 31) / 32, (len + 31) / 32), block(32, 8);
+    k_plane_to_col<<<grid, block, 0, st>>>(src, d.stage, len, nc);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(dst, d.stage, (size_t)len * nc * sizeof(double2), cudaMemcpyDeviceToHost, st);
+}
+
+cudaError_t instance_upload(DevInstance &d, const double *u1, const double *u2, const double *u3, const double *p,
+                            cudaStream_t st)
+{
+    const HostSetup &s = d.hs;
+    Inst &I = d.inst;
+    cudaError_t e;
+    if ((e = upload_field(d, u1, I.U1, s.nyu + 2, st)) != cudaSuccess) return e;
+    if ((e = upload_field(d, u2, I.U2, s.nyv + 2, st)) != cudaSuccess) return e;
+    if ((e = upload_field(d, u3, I.U3, s.nyu + 2, st)) != cudaSuccess) return e;
+    if ((e = upload_field(d, p, I.P, s.nyu, st)) != cudaSuccess) return e;
+    const size_t npc = (size_t)s.nyu * s.nc * sizeof(double2);
+    // Nu = 0 before the first step (littleharsh.f90:127-129)
+    if ((e = cudaMemsetAsync(I.NU1, 0, npc, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(I.NU2, 0, npc, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(I.NU3, 0, npc, st)) != cudaSuccess) return e;
+    double sc[SC_COUNT] = {0};
+    sc[SC_T] = 0.0;
+    sc[SC_DT] = d.desc.dt_mode == LH_DT_FIXED ? d.desc.dt : 0.0;
+    sc[SC_MPGX] = d.desc.mpgx;
+    const double q = u1 ? flowrate_host(s, u1) : 0.0;
+    sc[SC_QX] = q;
+    sc[SC_QXT] = q;  // getini: QxT = Qx for the constant flow-rate mode
+    if ((e = cudaMemcpyAsync(I.sc, sc, sizeof(sc), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(I.err, 0, sizeof(int), st)) != cudaSuccess) return e;
+    return cudaStreamSynchronize(st);
+}
+
+cudaError_t instance_download(DevInstance &d, double *u1, double *u2, double *u3, double *p, cudaStream_t st)
+{
+    const HostSetup &s = d.hs;
+    const Inst &I = d.inst;
+    cudaError_t e = cudaSuccess;
+    if (u1 && (e = download_field(d, I.U1, s.nyu + 2, u1, st)) != cudaSuccess) return e;
+    if (u2 && (e = download_field(d, I.U2, s.nyv + 2, u2, st)) != cudaSuccess) return e;
+    if (u3 && (e = download_field(d, I.U3, s.nyu + 2, u3, st)) != cudaSuccess) return e;
+    if (p && (e = download_field(d, I.P, s.nyu, p, st)) != cudaSuccess) return e;
+    return cudaStreamSynchronize(st);
+}
+
+// ---------------------------------------------------------------------------
+cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, const Tiles &t)
+{
+    plan_free(p);
+    p.tiles = t;
+    p.ninst = (int)insts.size();
+    int rounds = 0;
+    int maxMx = 0, maxMz = 0;
+    for (auto *d : insts) {
+        rounds = std::max(rounds, (d->hs.nyu + d->inst.chunk - 1) / d->inst.chunk);
+        maxMx = std::max(maxMx, d->hs.Mx);
+        maxMz = std::max(maxMz, d->hs.Mz);
+    }
+    p.zinv.assign(rounds, {});
+    p.xprod.assign(rounds, {});
+    p.zfwd.assign(rounds, {});
+    p.column.clear();
+    for (int q = 0; q < (int)insts.size(); q++) {
+        const HostSetup &s = insts[q]->hs;
+        const int chunk = insts[q]->inst.chunk;
+        const int nbz = (s.nxh + t.bc_zinv - 1) / t.bc_zinv;
+        const int nbx = (s.Mz + t.br_x - 1) / t.br_x;
+        const int nbf = (s.nxh + t.bc_zfwd - 1) / t.bc_zfwd;
+        for (int j = 1; j <= s.nyu; j++) {
+            const int r = (j - 1) / chunk, slot = (j - 1) % chunk;
+            for (int f = 0; f < kNumProducts; f++)
+                for (int b = 0; b < nbz; b++) p.zinv[r].push_back({q, j, slot, f * nbz + b});
+            for (int b = 0; b < nbx; b++) p.xprod[r].push_back({q, j, slot, b});
+            for (int b = 0; b < nbf; b++) p.zfwd[r].push_back({q, j, slot, b});
+        }
+        for (int b = 0; b < (s.nc + 127) / 128; b++) p.column.push_back({q, b, 0, 0});
+    }
+    std::vector<Work> all;
+    for (int r = 0; r < rounds; r++) {
+        p.off_zinv.push_back(all.size());
+        all.insert(all.end(), p.zinv[r].begin(), p.zinv[r].end());
+        p.off_xprod.push_back(all.size());
+        all.insert(all.end(), p.xprod[r].begin(), p.xprod[r].end());
+        p.off_zfwd.push_back(all.size());
+        all.insert(all.end(), p.zfwd[r].begin(), p.zfwd[r].end());
+    }
+    p.off_column = all.size();
+    all.insert(all.end(), p.column.begin(), p.column.end());
+    cudaError_t e = cudaMalloc(&p.d_work, all.size() * sizeof(Work));
+    if (e != cudaSuccess) {
+        p.d_work = nullptr;
+        return e;
+    }
+    e = cudaMemcpy(p.d_work, all.data(), all.size() * sizeof(Work), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
+    p.sm_zinv = smem_zinv(t, maxMz);
+    p.sm_x = smem_x(t, maxMx);
+    p.sm_zfwd = smem_zfwd(t, maxMz);
+    if ((e = cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.sm_zinv)) !=
+        cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(k_xprod, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.sm_x)) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.sm_zfwd)) !=
+        cudaSuccess)
+        return e;
+    return cudaSuccess;
+}
+
+void plan_free(Plan &p)
+{
+    if (p.d_work) cudaFree(p.d_work);
+    p.d_work = nullptr;
+    p.off_zinv.clear();
+    p.off_xprod.clear();
+    p.off_zfwd.clear();
+}
+
+cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl_any, cudaStream_t st)
+{
+    const Tiles &t = p.tiles;
+    for (size_t r = 0; r < p.zinv.size(); r++) {
+        k_zinv<<<(unsigned)p.zinv[r].size(), t.threads, p.sm_zinv, st>>>(d_insts, p.d_work + p.off_zinv[r],
+                                                                         t.bc_zinv);
+        k_xprod<<<(unsigned)p.xprod[r].size(), t.threads, p.sm_x, st>>>(d_insts, p.d_work + p.off_xprod[r], t.br_x,
+                                                                        (kRK == 1 && cfl_any) ? 1 : 0);
+        k_zfwd<<<(unsigned)p.zfwd[r].size(), t.threads, p.sm_zfwd, st>>>(d_insts, p.d_work + p.off_zfwd[r],
+                                                                         t.bc_zfwd);
+    }
+    if (kRK == 1) k_dt<<<p.ninst, 256, 0, st>>>(d_insts, p.ninst);
+    k_column<<<(unsigned)p.column.size(), 128, 0, st>>>(d_insts, p.d_work + p.off_column, kRK);
+    return cudaGetLastError();
+}
+
+}  // namespace lh

@@ -1,0 +1,68 @@
+// Engine internals shared by the single-instance context and the batch:
+// device memory of one instance and the launch plan of a substep.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "lh_core.cuh"
+#include "lh_setup.h"
+
+namespace lh {
+
+// Launch shapes of the plane pipeline and the column pass.
+struct Tiles {
+    int bc_zinv = 8;   // x modes per z-inverse CTA
+    int br_x = 2;      // z rows per x-transform CTA
+    int bc_zfwd = 1;   // x modes per z-forward CTA
+    int threads = 256; // threads per plane CTA
+    int chunk = 32;    // planes per staging chunk
+};
+
+Tiles default_tiles(int Mx, int Mz, int nxh, int nyu);
+size_t smem_zinv(const Tiles &t, int Mz);
+size_t smem_x(const Tiles &t, int Mx);
+size_t smem_zfwd(const Tiles &t, int Mz);
+
+// Device memory of one instance.  All buffers come from one allocation.
+struct DevInstance {
+    HostSetup hs;
+    lh_grid_desc desc{};
+    Inst inst{};           // host copy with device pointers
+    void *block = nullptr; // the allocation
+    size_t bytes = 0;
+    double2 *stage = nullptr;  // layout-transform staging (one field)
+    size_t stage_elems = 0;
+};
+
+// Bytes one instance needs for a staging chunk of `chunk` planes.
+size_t instance_bytes(const HostSetup &hs, int chunk);
+// Allocate and fill the device arrays of an instance (synchronous).
+cudaError_t instance_alloc(DevInstance &d, int chunk, cudaStream_t st);
+void instance_free(DevInstance &d);
+// Upload / download the four state fields in the reference column layout.
+cudaError_t instance_upload(DevInstance &d, const double *u1, const double *u2, const double *u3, const double *p,
+                            cudaStream_t st);
+cudaError_t instance_download(DevInstance &d, double *u1, double *u2, double *u3, double *p, cudaStream_t st);
+cudaError_t download_field(const DevInstance &d, const double2 *src, int len, double *dst, cudaStream_t st);
+
+// Work tables for a set of instances sharing launches.
+struct Plan {
+    std::vector<std::vector<Work>> zinv, xprod, zfwd;  // per chunk round
+    std::vector<Work> column;
+    Work *d_work = nullptr;  // all tables back to back
+    std::vector<size_t> off_zinv, off_xprod, off_zfwd;
+    size_t off_column = 0;
+    Tiles tiles;
+    size_t sm_zinv = 0, sm_x = 0, sm_zfwd = 0;
+    int ninst = 0;
+};
+
+cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, const Tiles &t);
+void plan_free(Plan &p);
+// Enqueue one substep of every instance of the plan.
+cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl_any, cudaStream_t st);
+
+}  // namespace lh

@@ -1,0 +1,26 @@
+// Kernel declarations (definitions in lh_plane.cu and lh_column.cu).
+#pragma once
+
+#include "lh_core.cuh"
+
+namespace lh {
+
+__global__ void k_zinv(const Inst *__restrict__ insts, const Work *__restrict__ work, int bc);
+__global__ void k_xprod(const Inst *__restrict__ insts, const Work *__restrict__ work, int br, int want_max);
+__global__ void k_zfwd(const Inst *__restrict__ insts, const Work *__restrict__ work, int bc);
+__global__ void k_plane_z_inv(const Inst *__restrict__ insts, double *planes, int bc);
+__global__ void k_plane_z_fwd(const Inst *__restrict__ insts, double *planes, int bc);
+__global__ void k_plane_x_inv(const Inst *__restrict__ insts, double *planes, int br);
+__global__ void k_plane_x_fwd(const Inst *__restrict__ insts, double *planes, int br);
+__global__ void k_plane_zero_row(const Inst *__restrict__ insts, double *planes);
+
+__global__ void k_column(const Inst *__restrict__ insts, const Work *__restrict__ work, int kRK);
+__global__ void k_dt(const Inst *__restrict__ insts, int ninst);
+__global__ void k_col_to_plane(const double2 *__restrict__ src, double2 *__restrict__ dst, int len, int nc);
+__global__ void k_plane_to_col(const double2 *__restrict__ src, double2 *__restrict__ dst, int len, int nc);
+__global__ void k_lusolu(const Inst *__restrict__ insts, int grid, int kRK, double dt, const double2 *rhs,
+                         double2 *u, double *fac);
+__global__ void k_lusolp(const Inst *__restrict__ insts, double2 *x);
+__global__ void k_divmax(const Inst *__restrict__ insts, double *out);
+
+}  // namespace lh

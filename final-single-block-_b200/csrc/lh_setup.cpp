@@ -1,0 +1,272 @@
+// Host set-up of one channel instance (see lh_setup.h).  The formulas follow
+// start.f90 line by line so the device operators see the same numbers the
+// reference would compute; integer powers use binary powering, which is how
+// a Fortran real**integer with a run-time exponent is evaluated.
+#include "lh_setup.h"
+
+#include <cmath>
+#include <sstream>
+
+namespace lh {
+
+static double powi(double x, int m)
+{
+    unsigned n = m < 0 ? (unsigned)(-m) : (unsigned)m;
+    double y = (n % 2) ? x : 1.0;
+    while (n >>= 1) {
+        x = x * x;
+        if (n % 2) y = y * x;
+    }
+    return m < 0 ? 1.0 / y : y;
+}
+
+// cffti1-style factorisation (cft_buff.f:141-163): try 3, 4, 2, 5, then odd
+// numbers; a factor 2 found after the first is moved to the front.
+static bool factor_fftpack(int n, const int try4[4], std::vector<int> &out)
+{
+    out.clear();
+    int nl = n, j = 0, ntry = 0;
+    std::vector<int> f;
+    while (nl != 1) {
+        j++;
+        ntry = j <= 4 ? try4[j - 1] : ntry + 2;
+        if (ntry > n) return false;
+        while (nl % ntry == 0) {
+            f.push_back(ntry);
+            nl /= ntry;
+            if (ntry == 2 && f.size() != 1) {
+                f.pop_back();
+                f.insert(f.begin(), 2);
+            }
+            if (nl == 1) break;
+        }
+    }
+    for (int p : f)
+        if (p != 2 && p != 3 && p != 4) return false;
+    out = f;
+    return true;
+}
+
+double flowrate_host(const HostSetup &s, const double *u1col)
+{
+    double Qu = 0.0;
+    for (int j = 1; j <= s.nyv + 1; j++) Qu = Qu + (s.yv[j] - s.yv[j - 1]) * u1col[2 * j];
+    return Qu;
+}
+
+std::string build_setup(const lh_grid_desc &d, HostSetup &s)
+{
+    std::ostringstream err;
+    if (d.Nx < 2 || d.Nz < 2 || d.Nx % 2 || d.Nz % 2) return "Nx and Nz must be even and >= 2";
+    if (d.ny < 5) return "ny must be >= 5";
+    if (!(d.Re > 0)) return "Re must be positive";
+    if (d.grid_type != LH_GRID_POLY && d.grid_type != LH_GRID_TANH) return "unknown grid_type";
+    if (d.dt_mode != LH_DT_CFL && d.dt_mode != LH_DT_FIXED) return "unknown dt_mode";
+    if (d.dt_mode == LH_DT_FIXED && !(d.dt > 0)) return "fixed dt must be positive";
+    if (d.flag_ctpress != 0 && d.flag_ctpress != 1) return "flag_ctpress must be 0 or 1";
+    s.Nx = d.Nx;
+    s.Nz = d.Nz;
+    // start.f90:135-136 Nspec = 2 Ngal / 3: only Ngal = 3 Nspec / 2 is exact
+    s.Mx = 3 * d.Nx / 2;
+    s.Mz = 3 * d.Nz / 2;
+    if ((3 * d.Nx) % 2 || (3 * d.Nz) % 2) return "3N/2 must be an integer";
+    s.nxh = d.Nx / 2 + 1;
+    s.nc = s.nxh * d.Nz;
+    s.nyv = d.ny - 2;
+    s.nyu = s.nyv + 1;
+    static const int tz[4] = {3, 4, 2, 5}, tx[4] = {4, 2, 3, 5};
+    if (!factor_fftpack(s.Mz, tz, s.radz)) {
+        err << "Ngal_z = " << s.Mz << " is not 2/3-smooth";
+        return err.str();
+    }
+    if (!factor_fftpack(s.Mx, tx, s.radx) || s.Mx % 2) {
+        err << "Ngal_x = " << s.Mx << " is not 2/3-smooth (rft_buff.f:308-311)";
+        return err.str();
+    }
+    if (s.radz.size() > 12 || s.radx.size() > 12) return "transform too long";
+
+    // ---- ygrid (start.f90:665-806)
+    const int nn = s.nyv + 1;
+    s.yu.assign(nn + 2, 0.0);
+    s.yv.assign(nn + 1, 0.0);
+    s.dthdyu.assign(nn + 2, 0.0);
+    s.dthdyv.assign(nn + 1, 0.0);
+    const double qqq = nn / 2.0;
+    if (d.grid_type == LH_GRID_POLY) {
+        const int ppp = d.ppp;
+        const double dyq = d.dyq;
+        if (ppp < 1) return "ppp must be >= 1";
+        const double bbb = (dyq - 1.0) / (qqq * (1.0 - powi(qqq, ppp - 1) +
+                                                 dyq * ((1.0 - qqq) * powi(qqq, ppp - 1) - powi(1.0 - qqq, ppp))));
+        const double aaa = (1.0 - bbb * powi(qqq, ppp)) / qqq;
+        s.yu[0] = aaa * (-1.0 + .5 - qqq) + bbb * powi(-1.0 + .5 - qqq, ppp);
+        for (int j = 0; j <= nn; j++) {
+            s.yv[j] = aaa * (j - qqq) + bbb * powi(j - qqq, ppp);
+            s.yu[j + 1] = aaa * (j + .5 - qqq) + bbb * powi(j + .5 - qqq, ppp);
+        }
+        s.dthdyu[0] = 1.0 / (aaa + ppp * bbb * powi(-1.0 + .5 - qqq, ppp - 1));
+        for (int j = 0; j <= nn; j++) {
+            s.dthdyv[j] = 1.0 / (aaa + ppp * bbb * powi(j - qqq, ppp - 1));
+            s.dthdyu[j + 1] = 1.0 / (aaa + ppp * bbb * powi(j + .5 - qqq, ppp - 1));
+        }
+    } else {
+        // tanh stretching: y(s) = tanh(g s)/tanh(g), s = (j - q)/q, with the
+        // analytic dtheta/dy = q tanh(g) / (g (1 - tanh^2(g s)))
+        const double g = d.gamma, tg = std::tanh(g);
+        if (!(g > 0)) return "gamma must be positive";
+        auto Y = [&](double x) { return std::tanh(g * (x - qqq) / qqq) / tg; };
+        auto T = [&](double x) {
+            const double th = std::tanh(g * (x - qqq) / qqq);
+            return 1.0 / (g * (1.0 - th * th) / (qqq * tg));
+        };
+        s.yu[0] = Y(-1.0 + .5);
+        s.dthdyu[0] = T(-1.0 + .5);
+        for (int j = 0; j <= nn; j++) {
+            s.yv[j] = Y((double)j);
+            s.yu[j + 1] = Y(j + .5);
+            s.dthdyv[j] = T((double)j);
+            s.dthdyu[j + 1] = T(j + .5);
+        }
+    }
+    const std::vector<double> &yu = s.yu, &yv = s.yv;
+    s.dyu2i.assign(3 * (nn + 2), 0.0);
+    s.dyv2i.assign(3 * (nn + 1), 0.0);
+    auto DU = [&](int r, int j) -> double & { return s.dyu2i[(r - 1) + 3 * j]; };
+    auto DV = [&](int r, int j) -> double & { return s.dyv2i[(r - 1) + 3 * j]; };
+    int j = 0;
+    DU(1, j) = 0.0;
+    DU(2, j) = -2.0 / ((yu[j + 1] - yu[j]) * (yu[j + 1] - yu[j]));
+    DU(3, j) = 1.0 / ((yu[j + 1] - yu[j]) * (yu[j + 1] - yu[j]));
+    DV(1, j) = 0.0;
+    DV(2, j) = -2.0 / ((yv[j + 1] - yv[j]) * (yv[j + 1] - yv[j]));
+    DV(3, j) = 1.0 / ((yv[j + 1] - yv[j]) * (yv[j + 1] - yv[j]));
+    for (j = 1; j <= nn - 1; j++) {
+        DU(1, j) = 2.0 / ((yu[j] - yu[j - 1]) * (yu[j + 1] - yu[j - 1]));
+        DU(2, j) = -2.0 / ((yu[j + 1] - yu[j]) * (yu[j] - yu[j - 1]));
+        DU(3, j) = 2.0 / ((yu[j + 1] - yu[j]) * (yu[j + 1] - yu[j - 1]));
+        DV(1, j) = 2.0 / ((yv[j] - yv[j - 1]) * (yv[j + 1] - yv[j - 1]));
+        DV(2, j) = -2.0 / ((yv[j + 1] - yv[j]) * (yv[j] - yv[j - 1]));
+        DV(3, j) = 2.0 / ((yv[j + 1] - yv[j]) * (yv[j + 1] - yv[j - 1]));
+    }
+    j = nn;
+    DU(1, j) = 2.0 / ((yu[j] - yu[j - 1]) * (yu[j + 1] - yu[j - 1]));
+    DU(2, j) = -2.0 / ((yu[j + 1] - yu[j]) * (yu[j] - yu[j - 1]));
+    DU(3, j) = 2.0 / ((yu[j + 1] - yu[j]) * (yu[j + 1] - yu[j - 1]));
+    DV(1, j) = 1.0 / ((yv[j] - yv[j - 1]) * (yv[j] - yv[j - 1]));
+    DV(2, j) = -2.0 / ((yv[j] - yv[j - 1]) * (yv[j] - yv[j - 1]));
+    DV(3, j) = 0.0;
+    j = nn + 1;
+    DU(1, j) = 1.0 / ((yu[j] - yu[j - 1]) * (yu[j] - yu[j - 1]));
+    DU(2, j) = -2.0 / ((yu[j] - yu[j - 1]) * (yu[j] - yu[j - 1]));
+    DU(3, j) = 0.0;
+    s.ddthetavi = 1.0;
+
+    // ---- def_k (start.f90:842-862)
+    s.kx.assign(s.nxh, 0.0);
+    s.k2x.assign(s.nxh, 0.0);
+    for (int i = 0; i <= d.Nx / 2; i++) {
+        s.kx[i] = d.alp * i;
+        s.k2x[i] = -((d.alp * i) * (d.alp * i));
+    }
+    s.kz.assign(d.Nz, 0.0);
+    s.k2z.assign(d.Nz, 0.0);
+    for (int k = 1; k <= d.Nz / 2; k++) {
+        s.kz[k - 1] = d.bet * (k - 1);
+        s.k2z[k - 1] = -((d.bet * (k - 1)) * (d.bet * (k - 1)));
+    }
+    for (int k = d.Nz / 2 + 1; k <= d.Nz; k++) {
+        s.kz[k - 1] = -(d.bet * (d.Nz - k + 1));
+        s.k2z[k - 1] = -((d.bet * (d.Nz - k + 1)) * (d.bet * (d.Nz - k + 1)));
+    }
+
+    // ---- weights and dtv (start.f90:476, 518-537)
+    const int nyu = s.nyu, nyv = s.nyv;
+    s.gw1 = -(yv[0] - yu[0]) / (yv[0] - yu[1]);
+    s.gw2 = (yu[nyu + 1] - yv[nyv + 1]) / (yv[nyv + 1] - yu[nyu]);
+    s.gwbc = (yu[0] - yv[0]) / (yu[1] - yv[0]);
+    s.gwi1 = (yu[0] - yu[1]) / (yv[0] - yu[1]);
+    s.gwi2 = (yu[nyu + 1] - yu[nyu]) / (yv[nyv + 1] - yu[nyu]);
+    s.dtv = d.Re / (-s.k2x[d.Nx / 2] - s.k2z[d.Nz / 2 - 1] + 4.0 / ((yv[1] - yv[0]) * (yv[1] - yv[0])));
+
+    // ---- LU_buildP + LU_decP (tridLU_3D.f90:224-297, 366-407)
+    const int ns = 1, ne = nyu, len = ne - ns + 1, nc = s.nc;
+    std::vector<double> Db(len + 2), Gb(len + 2), Dt(len + 2), Gt(len + 2);
+    auto V = [&](std::vector<double> &a, int jj) -> double & { return a[jj - ns + 1]; };
+    for (int jj = ns; jj <= ne; jj++) {
+        V(Db, jj - 1) = -s.ddthetavi * s.dthdyu[jj];
+        V(Gb, jj) = -s.ddthetavi * s.dthdyv[jj];
+        V(Dt, jj) = s.ddthetavi * s.dthdyu[jj];
+        V(Gt, jj + 1) = s.ddthetavi * s.dthdyv[jj];
+    }
+    s.DG1.assign(nyu + 1, 0.0);
+    for (int jj = ns + 1; jj <= ne; jj++) s.DG1[jj] = V(Db, jj - 1) * V(Gb, jj - 1);
+    s.DG2.assign((size_t)len * nc, 0.0);
+    s.DG3.assign((size_t)len * nc, 0.0);
+    std::vector<double> a1(len + 1), a2(len + 1), a3(len + 1);
+    for (int col = 0; col < nc; col++) {
+        const int i = col % s.nxh, kr = col / s.nxh;
+        const double k2x = s.k2x[i], k2z = s.k2z[kr];
+        a2[ns] = (V(Dt, ns) * V(Gb, ns)) + k2x + k2z;
+        a3[ns] = (V(Dt, ns) * V(Gt, ns + 1));
+        a1[ns] = 0.0;
+        a2[ne] = (V(Db, ne - 1) * V(Gt, ne)) + k2x + k2z;
+        a1[ne] = (V(Db, ne - 1) * V(Gb, ne - 1));
+        a3[ne] = 0.0;
+        for (int jj = ns + 1; jj <= ne - 1; jj++) {
+            a2[jj] = (V(Db, jj - 1) * V(Gt, jj)) + (V(Dt, jj) * V(Gb, jj)) + k2x + k2z;
+            a1[jj] = (V(Db, jj - 1) * V(Gb, jj - 1));
+            a3[jj] = (V(Dt, jj) * V(Gt, jj + 1));
+        }
+        if (col == 0) {  // gauge row of the (0,0) mode (tridLU_3D.f90:276-280)
+            a1[ns] = 0.0;
+            a2[ns] = 1.0 / ((yu[1 + 1] - yu[1]) * (yu[1 + 1] - yu[1]));
+            a3[ns] = 0.0;
+        }
+        a2[ns] = 1.0 / a2[ns];
+        for (int jj = ns + 1; jj <= ne; jj++) {
+            a3[jj - 1] = a3[jj - 1] * a2[jj - 1];
+            a2[jj] = 1.0 / (a2[jj] - a1[jj] * a3[jj - 1]);
+        }
+        for (int jj = ns; jj <= ne; jj++) {
+            s.DG2[(size_t)(jj - 1) * nc + col] = a2[jj];
+            s.DG3[(size_t)(jj - 1) * nc + col] = a3[jj];
+        }
+    }
+
+    // ---- twiddles: z with the rotation recurrence of cffti1
+    // (cft_buff.f:166-179), x with direct cos/sin as rffti1 does
+    s.twz.assign(2 * s.Mz, 0.0);
+    {
+        const double tpi = 8.0 * std::atan(1.0);
+        const double arg1 = tpi / (double)(float)s.Mz;
+        const double dc = std::cos(arg1), ds = std::sin(arg1);
+        std::vector<double> wa(2 * s.Mz);
+        wa[0] = dc;
+        wa[1] = ds;
+        for (int ii = 4; ii <= 2 * s.Mz; ii += 2) {
+            wa[ii - 2] = dc * wa[ii - 4] - ds * wa[ii - 3];
+            wa[ii - 1] = ds * wa[ii - 4] + dc * wa[ii - 3];
+        }
+        s.twz[0] = 1.0;
+        s.twz[1] = 0.0;
+        for (int t = 1; t < s.Mz; t++) {
+            s.twz[2 * t] = wa[2 * t - 2];
+            s.twz[2 * t + 1] = wa[2 * t - 1];
+        }
+    }
+    s.twx.assign(2 * s.Mx, 0.0);
+    {
+        const double tpi = 2.0 * std::atan2(0.0, -1.0);
+        const double argh = tpi / (double)(float)s.Mx;
+        for (int t = 0; t < s.Mx; t++) {
+            const double arg = (double)t * argh;
+            s.twx[2 * t] = std::cos(arg);
+            s.twx[2 * t + 1] = std::sin(arg);
+        }
+        s.twx[0] = 1.0;
+        s.twx[1] = 0.0;
+    }
+    return std::string();
+}
+
+}  // namespace lh

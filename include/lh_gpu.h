@@ -1,0 +1,166 @@
+/*
+ * lh_gpu.h -- C ABI of the B200 (sm_100a) FP64 time-step engine for the
+ * LittleHarsh channel DNS.
+ *
+ * The entry points replace, one for one, the reference subroutines that sit
+ * under the Fortran main loop (reference file:line given beside each).  All
+ * arrays use the reference's own layouts so a Fortran caller can pass its
+ * arrays unchanged through iso_c_binding:
+ *
+ *   column fields   complex(8) x(jlim(1,grid):jlim(2,grid), column), j fastest,
+ *                   interleaved (re, im) doubles.  Column order is the
+ *                   reference's np=1 order: k = 1..Nz (z mode), i = 0..Nx/2
+ *                   inner (start.f90:964-981).
+ *                     u1, u3 : j = 0 .. nyu+1   (nyu = ny-1)
+ *                     u2     : j = 0 .. nyv+1   (nyv = ny-2)
+ *                     p      : j = 1 .. nyu
+ *   plane arrays    real(8) xPL(Ngal_x+2, Ngal_z), x fastest, (re, im) pairs
+ *                   for spectral planes (FOU3D.f90:734).
+ *
+ * Every function returns 0 on success and a negative LH_E* code on failure;
+ * lh_last_error() gives a message.  Device faults are reported through a
+ * device error word, never by trapping.  One caller thread per context.
+ */
+#ifndef LH_GPU_H
+#define LH_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LH_OK 0
+#define LH_EINVAL -1   /* bad argument or unsupported size */
+#define LH_ECUDA -2    /* CUDA runtime error */
+#define LH_ENOMEM -3   /* device allocation failed / over budget */
+#define LH_EDEVICE -4  /* device-side error word set (non-finite state, ...) */
+#define LH_ESTATE -5   /* call out of order (no state uploaded, ...) */
+
+#define LH_GRID_POLY 0 /* reference polynomial grid, start.f90:665-806 */
+#define LH_GRID_TANH 1 /* tanh(gamma s)/tanh(gamma) stretching (extension) */
+
+#define LH_DT_CFL 0    /* reference CFL rule at kRK=1, FOU3D.f90:290-303 */
+#define LH_DT_FIXED 1  /* fixed dt (extension used by the benchmark configs) */
+
+/* Instance description: the values start.f90 reads from input.in
+ * (start.f90:85-252) plus the two extensions above. */
+typedef struct lh_grid_desc {
+    int Nx, Nz;          /* Fourier modes Nspec_x, Nspec_z (Ngal = 3N/2) */
+    int ny;              /* input ny: v faces 0..ny-1 */
+    double Re;           /* bulk Reynolds number */
+    double alp, bet;     /* box wavenumbers, Lx = 2pi/alp, Lz = 2pi/bet */
+    double mpgx;         /* mean pressure gradient (flpress = 1) */
+    int flag_ctpress;    /* 1: constant pressure gradient, 0: constant flow rate */
+    int grid_type;       /* LH_GRID_* */
+    double dyq;          /* poly grid: dymax/dymin */
+    int ppp;             /* poly grid: exponent */
+    double gamma;        /* tanh grid: stretching */
+    int dt_mode;         /* LH_DT_* */
+    double CFL;          /* CFL number (LH_DT_CFL) */
+    double dt;           /* time step (LH_DT_FIXED) */
+} lh_grid_desc;
+
+typedef struct lh_ctx lh_ctx;
+
+/* Sizes of one instance: [Nx, Nz, Mx, Mz, nyu, nyv, ncols, igal, kgal] */
+typedef struct lh_sizes {
+    int Nx, Nz, Mx, Mz, nyu, nyv, ncols, igal, kgal;
+} lh_sizes;
+
+/* ---- context: replaces start() set-up, start.f90:53-662 -------------- */
+int lh_ctx_create(const lh_grid_desc *desc, lh_ctx **out);
+int lh_ctx_destroy(lh_ctx *ctx);
+const char *lh_last_error(const lh_ctx *ctx);
+int lh_get_sizes(const lh_ctx *ctx, lh_sizes *out);
+/* Grid arrays as built on the host: which = 0 yu, 1 yv, 2 dthdyu, 3 dthdyv
+ * (lengths nyu+2 / nyv+2).  Returns the element count. */
+int lh_get_grid(const lh_ctx *ctx, int which, double *out, int cap);
+
+/* Host-only set-up query (needs no GPU): the same arrays as lh_get_grid for a
+ * description, or, for which = 4, the scalars [gw1, gw2, gw_bc, gwi1, gwi2,
+ * dtv] (start.f90:476, 518-537).  Returns the element count or LH_EINVAL. */
+int lh_host_grid(const lh_grid_desc *desc, int which, double *out, int cap);
+
+/* ---- state: replaces getini/read_in (start.f90:1221-1997) ------------- */
+/* Host arrays in the reference column layout (see above).  p may be NULL
+ * (zero pressure).  Resets Nu (littleharsh.f90:127-129), t and iter. */
+int lh_upload_state(lh_ctx *ctx, const double *u1, const double *u2,
+                    const double *u3, const double *p);
+int lh_download_state(lh_ctx *ctx, double *u1, double *u2, double *u3,
+                      double *p);
+/* Nu1, Nu2, Nu3 (interior rows) of the last substep, column layout:
+ * Nu1/Nu3 j = 1..nyu, Nu2 j = 1..nyv.  Any pointer may be NULL. */
+int lh_download_nu(lh_ctx *ctx, double *nu1, double *nu2, double *nu3);
+
+/* ---- the RK3 step: replaces the loop body littleharsh.f90:165-231 ---- */
+/* One substep kRK = 1..3: RHS0_u1/2/3, nonlinear, solveU x3,
+ * flowrate correction (flag_ctpress = 0), solveP, v_corr. */
+int lh_substep(lh_ctx *ctx, int kRK);
+/* nsteps full RK3 steps (captured once in a CUDA graph and replayed). */
+int lh_step(lh_ctx *ctx, int nsteps);
+/* t, dt, iter, mpgx, Qx (flow rate of the (0,0) mode) */
+int lh_get_scalars(lh_ctx *ctx, double *t, double *dt, int *iter,
+                   double *mpgx, double *Qx);
+/* Host-buffer step for callers that keep the state on the host: upload,
+ * nsteps RK3 steps, download (the Fortran drop-in call). */
+int lh_step_host(lh_ctx *ctx, double *u1, double *u2, double *u3, double *p,
+                 int nsteps);
+int lh_synchronize(lh_ctx *ctx);
+/* The CUDA stream (cudaStream_t) every call of this context is ordered on. */
+int lh_get_stream(lh_ctx *ctx, void **stream);
+/* Runs nsteps RK3 steps launch by launch with CUDA events around every
+ * kernel and returns, per kernel class (0 z-inverse, 1 x-products,
+ * 2 z-forward, 3 dt, 4 column), the summed milliseconds and launch counts. */
+int lh_profile(lh_ctx *ctx, int nsteps, double *ms, int *launches);
+/* max |div| after the last projection (error(), littleharsh.f90:370-409) */
+int lh_error_div(lh_ctx *ctx, double *err);
+
+/* ---- nonlinear-term intermediates of the last substep (parity) -------- */
+/* which: 0 Nu1 x/z part, 1 Nu2 x/z part, 2 Nu3 x/z part (FOU3D.f90:259-261
+ * before the y-flux sum), 3 uv_f (j=0..nyv+1), 4 vv_c (j=0..nyu+1),
+ * 5 wv_f (j=0..nyv+1).  Column layout.  Returns the element count. */
+int lh_get_intermediate(lh_ctx *ctx, int which, double *out, size_t cap);
+
+/* ---- plane transforms: replace four_to_phys_u (FOU3D.f90:653-679) and --
+ * phys_to_four_du (FOU3D.f90:1654-1672), i.e. cft/rft on a plane.
+ * nplanes planes of igal*kgal doubles, host pointers, in place. */
+int lh_four_to_phys(lh_ctx *ctx, double *planes, int nplanes);
+int lh_phys_to_four(lh_ctx *ctx, double *planes, int nplanes);
+
+/* ---- tridiagonal solves: replace LUsolU (tridLU_3D.f90:38-94, with
+ * LU_build :163-221 and LU_dec :327-364) and LUsolP (tridLU_3D.f90:98-132
+ * with the DG factors of LU_buildP/LU_decP :224-297, :366-407).
+ * grid: 2 = u/w (j = 0..nyu+1), 1 = v (j = 0..nyv+1).  beta = bRK*dt/Re is
+ * taken from kRK and dt.  Column layout, host pointers. */
+int lh_lusolu(lh_ctx *ctx, int grid, int kRK, double dt, const double *rhs,
+              double *u);
+int lh_lusolp(lh_ctx *ctx, double *x);
+
+/* ---- batched / served instances ------------------------------------- */
+typedef struct lh_batch lh_batch;
+/* A batch owns many independent instances of uneven size that advance in
+ * shared launches.  HBM budget in bytes (0 = no limit). */
+int lh_batch_create(size_t hbm_budget, lh_batch **out);
+int lh_batch_destroy(lh_batch *b);
+const char *lh_batch_last_error(const lh_batch *b);
+/* Bytes of device memory one instance of this description needs. */
+size_t lh_instance_bytes(const lh_grid_desc *desc);
+/* Admit an instance (returns its slot id >= 0) with its initial state in
+ * the column layout; LH_ENOMEM when the budget is exhausted. */
+int lh_batch_add(lh_batch *b, const lh_grid_desc *desc, const double *u1,
+                 const double *u2, const double *u3, const double *p,
+                 int *slot);
+int lh_batch_remove(lh_batch *b, int slot);
+/* Advance every live instance by nsteps RK3 steps in shared launches. */
+int lh_batch_step(lh_batch *b, int nsteps);
+int lh_batch_download(lh_batch *b, int slot, double *u1, double *u2,
+                      double *u3, double *p);
+int lh_batch_scalars(lh_batch *b, int slot, double *t, double *dt, int *iter);
+int lh_batch_count(const lh_batch *b);
+int lh_batch_synchronize(lh_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LH_GPU_H */

@@ -472,11 +472,21 @@ int lho_field_len(const lho_ctx *c, int f)
     return n;
 }
 
+static double flowrate_im(const lho_ctx *c, const double *u1col);
+
 void lho_set_field(lho_ctx *c, int f, const double *src)
 {
     int n;
     double *p = field_ptr(c, f, &n);
     if (p) memcpy(p, src, sizeof(double) * n);
+    if (f == 0) {
+        /* getini after read_in (start.f90:1258-1267): Qx of the initial
+         * field; the constant flow-rate mode keeps it as its target QxT */
+        c->Qx = flowrate_im(c, c->u1);
+        if (c->prm.flag_ctpress != 1) c->QxT = c->Qx;
+        c->t = 0.0;
+        c->iter = 0;
+    }
 }
 
 void lho_get_field(const lho_ctx *c, int f, double *dst)
