@@ -1,0 +1,308 @@
+"""Throughput benchmark of the channel-DNS time step on B200.
+
+Workload (one instance per GPU): 128x128 Fourier modes (192x192 physical
+with the 3/2 pad), ny = 153 on the reference's stretched grid, Re_tau = 180
+(Re = 180/sqrt(3.0675e-3)), fixed dt = 5e-4, seeded perturbed-laminar
+initial state.  A step is one RK3 step (3 substeps).  The metric counts
+grid points Nx*Nz*ny times substeps per second over the whole job.
+
+  value  device-resident state, one CUDA graph per step, CUDA events on the
+         engine's stream, max over ranks
+  e2e    the host-buffer C-ABI call lh_step_host: pinned host arrays in the
+         reference column layout are uploaded, stepped and downloaded every
+         step
+  --impl reference   the reference algorithm on the host cores (the C
+         restatement, all threads), on a bounded sample of the same workload
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+N > 1 runs under torchrun, one independent instance per rank (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "final-single-block-_b200"))
+
+METRIC = "FP64 grid-pt·substeps/s: served batch vs plain 1-instance on B200; p50/p99 lat"
+UNIT = "grid-pt*substeps/s"
+RE_TAU = 180.0
+MPGX = -3.0675e-3
+
+
+def workload_desc():
+    from lh_b200 import Desc, re_from_retau
+    return Desc(Nx=128, Nz=128, ny=153, Re=re_from_retau(RE_TAU, MPGX), mpgx=MPGX, dt_mode=1, dt=5e-4)
+
+
+def config_dict(desc, n_gpus):
+    return {
+        "workload": "plain drop-in, one channel instance per GPU: Nx=Nz=128 modes (192x192 physical, 3/2 pad), "
+                    "ny=153 polynomial-stretched y (dyq=10, p=5), Re_tau=180, dt=5e-4, RK3, seeded "
+                    "perturbed-laminar initial state",
+        "Nx": desc.Nx, "Nz": desc.Nz, "ny": desc.ny, "Re": desc.Re, "dt": desc.dt,
+        "grid_points": desc.points(), "substeps_per_step": 3,
+        "instances_per_gpu": 1, "parallelism": f"replicas x{n_gpus}",
+        "l2": "state and per-substep traffic (~0.45 GB resident) exceed the 126 MB L2; no flush",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) >= 9 and r[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the column pass from the committed ncu capture."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+def cpu_rate(desc, sample_steps: int, threads: int):
+    """Reference algorithm on the host (oracle, OpenMP) -> (rate, seconds, cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from lh_b200 import grids, perturbed_laminar
+    cfg = O.Config(Nx=desc.Nx, Nz=desc.Nz, ny=desc.ny, Re=desc.Re, mpgx=desc.mpgx, dt_mode=O.DT_FIXED,
+                   dt_fixed=desc.dt, nthreads=threads)
+    yu, yv = grids(desc)
+    ic = perturbed_laminar(desc, 20260002, yu, yv)
+    o = O.Oracle(cfg, threaded=True)
+    o.load_state(*ic)
+    o.step(1)  # warm caches and page in
+    t0 = time.perf_counter()
+    o.step(sample_steps)
+    dt = time.perf_counter() - t0
+    return desc.points() * 3 * sample_steps / dt, dt
+
+
+def run_reference(args, rank, world):
+    desc = workload_desc()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    steps = max(1, args.steps)
+    warm = max(0, min(args.warmup, 1))
+    # bounded sample: each timed step is one RK3 step of the full workload
+    sample = min(steps, 3)
+    rate, secs = cpu_rate(desc, sample, threads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
+        "steps": sample, "warmup": warm, "ms_per_step": 1e3 * secs / sample, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(desc, world),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{sample} RK3 steps of the full 128x128x153 workload, C restatement "
+                                   f"of the reference (OpenMP, {threads} threads); the Fortran build needs "
+                                   f"a Fortran compiler and MPI, absent here"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def column_alg_bytes(desc):
+    """Algorithmic bytes of one column-pass launch: the 13 fields it must read
+    (u1 u2 u3 p, Nu of the previous substep x3, x/z parts of Nu x3, y-flux
+    spectra x3) and the 7 it must write (u1 u2 u3 p, Nu x3), 16 B per complex
+    entry, ncols x ny entries each."""
+    F = 16 * desc.ncols * desc.ny
+    return 20 * F
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from lh_b200 import Engine, grids, perturbed_laminar
+    torch.cuda.set_device(local_rank)
+    desc = workload_desc()
+    yu, yv = grids(desc)
+    ic = perturbed_laminar(desc, 20260002 + 1000 * rank, yu, yv)
+    e = Engine(desc)
+    e.upload(*ic)
+    st = torch.cuda.ExternalStream(e.stream())
+    W, K = args.warmup, args.steps
+    e.step(W)
+    e.synchronize()
+    pts_sub = desc.points() * 3
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+        tdist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        ev0.record(st)
+        e.step(K)
+        ev1.record(st)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    e.synchronize()  # error word: non-finite state fails the run
+    tmax = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        tdist.all_reduce(tmax, op=tdist.ReduceOp.MAX)
+    ms_max = float(tmax.item())
+    value = world * pts_sub * K / (ms_max * 1e-3)
+    launches_per_step = None
+
+    # per-kernel breakdown with CUDA events on the engine's stream
+    prof = e.profile(2)
+    launches_per_step = sum(n for _, n in prof.values()) // 2
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    col_ms, col_n = prof["column"]
+    col_avg_ms = col_ms / col_n
+    hbm, src = peaks()
+    alg = column_alg_bytes(desc)
+    achieved = alg / (col_avg_ms * 1e-3) / 1e9
+    traffic = ncu_traffic().get("column_dram_bytes_per_launch")
+
+    # end to end through the host-buffer call
+    nu, nv, nc = desc.nyu, desc.nyv, desc.ncols
+    shapes = [(nc, nu + 2), (nc, nv + 2), (nc, nu + 2), (nc, nu)]
+    host = []
+    for shp, src_arr in zip(shapes, ic):
+        t = torch.empty(int(np.prod(shp)) * 2, dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = np.ascontiguousarray(src_arr).view(np.float64).ravel()
+        host.append(t)
+    addrs = [t.data_ptr() for t in host]
+    nbytes = sum(t.numel() * 8 for t in host)
+    Ke = max(2, min(K, 10))
+    e.step_host(addrs, 1)  # warm
+    if dist:
+        tdist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(Ke):
+        e.step_host(addrs, 1)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        tdist.all_reduce(te, op=tdist.ReduceOp.MAX)
+    e2e_val = world * pts_sub * Ke / float(te.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        rate, secs = cpu_rate(desc, 2, threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"2 RK3 steps of the same 128x128x153 workload on the host, C restatement of the "
+                         f"reference path (OpenMP, {threads} threads), {secs:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": config_dict(desc, world),
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+            "gpu_launches": launches_per_step * K,
+            "roofline": {"bound": "hbm", "kernel": "k_column (column pass)", "achieved": achieved, "peak": hbm,
+                         "peak_source": src, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                         "alg_bytes_per_launch": alg, "avg_launch_ms": col_avg_ms},
+            "kernels_ms_per_step": {k: v[0] / 2 for k, v in prof.items()},
+            "dominant_kernel": dom[0],
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    e.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus and world == 1 and args.gpus > 1:
+        print(json.dumps({"error": "run N>1 under torchrun"}))
+        sys.exit(2)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as tdist
+            tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -183,7 +183,9 @@ def test_fixed_dt_synthetic_ic(grid_type, ctpress):
     errs = {f: rel_l2(g[f], r[f]) for f in FIELDS}
     assert all(v <= 1e-9 for v in errs.values()), errs
     if ctpress == 0:
-        assert abs(e.scalars()["mpgx"] - o.scalar(3)) <= 1e-10 * abs(o.scalar(3))
+        # mpgx accumulates g = (QxT - Qx0)/Qx1, a difference of nearly equal
+        # flow rates, so its relative error is larger than the fields'
+        assert abs(e.scalars()["mpgx"] - o.scalar(3)) <= 1e-8 * abs(o.scalar(3))
 
 
 def test_one_step_128():
