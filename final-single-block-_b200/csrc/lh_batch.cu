@@ -182,8 +182,7 @@ static int rebuild(lh_batch *b)
         b->d_insts_cap = hi.size();
     }
     BCK(cudaMemcpy(b->d_insts, hi.data(), hi.size() * sizeof(Inst), cudaMemcpyHostToDevice), "instance table");
-    Tiles t = default_tiles(maxMx, maxMz, maxnxh, maxnyu);
-    BCK(plan_build(b->plan, v, t), "plan");
+    BCK(plan_build(b->plan, v), "plan");
     BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal), "capture");
     cudaError_t el = cudaSuccess;
     for (int k = 1; k <= 3 && el == cudaSuccess; k++) el = launch_substep(b->plan, b->d_insts, k, b->any_cfl, b->st);

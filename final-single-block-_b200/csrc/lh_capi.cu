@@ -3,6 +3,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -67,10 +68,11 @@ extern "C" int lh_ctx_create(const lh_grid_desc *desc, lh_ctx **out)
     }
     const HostSetup &s = c->dev.hs;
     Tiles t = default_tiles(s.Mx, s.Mz, s.nxh, s.nyu);
+    const char *gen = getenv("LH_GENERIC_FFT");
     e = instance_alloc(c->dev, t.chunk, c->st);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_inst, sizeof(Inst));
     if (e == cudaSuccess) e = cudaMemcpy(c->d_inst, &c->dev.inst, sizeof(Inst), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = plan_build(c->plan, {&c->dev}, t);
+    if (e == cudaSuccess) e = plan_build(c->plan, {&c->dev}, gen && gen[0] == '1');
     if (e != cudaSuccess) {
         int code = e == cudaErrorMemoryAllocation ? LH_ENOMEM : LH_ECUDA;
         lh_ctx_destroy(c);
@@ -375,52 +377,19 @@ extern "C" int lh_profile(lh_ctx *c, int nsteps, double *ms, int *launches)
 {
     if (!c || !ms || !launches || nsteps < 1) return LH_EINVAL;
     if (!c->have_state) return fail(c, LH_ESTATE, "no state uploaded");
-    for (int k = 0; k < 5; k++) {
-        ms[k] = 0.0;
-        launches[k] = 0;
-    }
-    const Plan &p = c->plan;
-    const Tiles &t = p.tiles;
-    const bool cfl = c->dev.desc.dt_mode == LH_DT_CFL;
-    cudaEvent_t ev[2];
-    CK(cudaEventCreate(&ev[0]), "event");
-    CK(cudaEventCreate(&ev[1]), "event");
-    auto timed = [&](int cls, auto &&launch) -> cudaError_t {
-        cudaEventRecord(ev[0], c->st);
-        launch();
-        cudaEventRecord(ev[1], c->st);
-        cudaError_t e = cudaEventSynchronize(ev[1]);
-        float f = 0.f;
-        cudaEventElapsedTime(&f, ev[0], ev[1]);
-        ms[cls] += f;
-        launches[cls] += 1;
-        return e == cudaSuccess ? cudaGetLastError() : e;
-    };
+    LaunchTimer t;
+    CK(cudaEventCreate(&t.ev[0]), "event");
+    CK(cudaEventCreate(&t.ev[1]), "event");
     cudaError_t e = cudaSuccess;
+    const bool cfl = c->dev.desc.dt_mode == LH_DT_CFL;
     for (int s = 0; s < nsteps && e == cudaSuccess; s++)
-        for (int kRK = 1; kRK <= 3 && e == cudaSuccess; kRK++) {
-            for (size_t r = 0; r < p.zinv.size() && e == cudaSuccess; r++) {
-                e = timed(0, [&] {
-                    k_zinv<<<(unsigned)p.zinv[r].size(), t.threads, p.sm_zinv, c->st>>>(c->d_inst, p.d_work + p.off_zinv[r], t.bc_zinv);
-                });
-                if (e == cudaSuccess)
-                    e = timed(1, [&] {
-                        k_xprod<<<(unsigned)p.xprod[r].size(), t.threads, p.sm_x, c->st>>>(
-                            c->d_inst, p.d_work + p.off_xprod[r], t.br_x, (kRK == 1 && cfl) ? 1 : 0);
-                    });
-                if (e == cudaSuccess)
-                    e = timed(2, [&] {
-                        k_zfwd<<<(unsigned)p.zfwd[r].size(), t.threads, p.sm_zfwd, c->st>>>(c->d_inst, p.d_work + p.off_zfwd[r], t.bc_zfwd);
-                    });
-            }
-            if (kRK == 1 && e == cudaSuccess) e = timed(3, [&] { k_dt<<<p.ninst, 256, 0, c->st>>>(c->d_inst, p.ninst); });
-            if (e == cudaSuccess)
-                e = timed(4, [&] {
-                    k_column<<<(unsigned)p.column.size(), 128, 0, c->st>>>(c->d_inst, p.d_work + p.off_column, kRK);
-                });
-        }
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
+        for (int k = 1; k <= 3 && e == cudaSuccess; k++) e = launch_substep(c->plan, c->d_inst, k, cfl, c->st, &t);
+    cudaEventDestroy(t.ev[0]);
+    cudaEventDestroy(t.ev[1]);
     if (e != cudaSuccess) return cuda_fail(c, e, "profile");
+    for (int k = 0; k < 5; k++) {
+        ms[k] = t.ms[k];
+        launches[k] = t.n[k];
+    }
     return LH_OK;
 }

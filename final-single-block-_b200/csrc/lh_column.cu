@@ -41,13 +41,48 @@ __device__ __forceinline__ RK rk_coeffs(int kRK)
 
 __device__ __forceinline__ double2 cscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
 
-__global__ void __launch_bounds__(128) k_column(const Inst *__restrict__ insts, const Work *__restrict__ work,
-                                                int kRK)
+// Per-thread asynchronous row prefetch.  Each thread streams the rows of
+// its own column through a ring of kStages shared-memory stages with
+// cp.async, so a sweep keeps kStages-1 rows of loads in flight while it
+// works on the current row; slots are [stage][slot][lane] so the 32 lanes of
+// a warp touch 512 contiguous bytes.
+constexpr int kColThreads = 32;
+constexpr int kStages = 8;
+constexpr int kSlotsA = 13, kSlotsB = 4, kSlotsC = 2, kSlotsD = 6;
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp16(double2 *s, const double2 *g)
 {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(s)), "l"(g));
+}
+__device__ __forceinline__ void cp8(double *s, const double *g)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(s)), "l"(g));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+struct Ring {
+    double2 *base;
+    int nslot, lane;
+    __device__ double2 *at(int stage, int slot) const { return base + ((stage * nslot + slot) * kColThreads + lane); }
+};
+
+size_t column_smem_bytes() { return (size_t)kStages * kSlotsA * kColThreads * sizeof(double2); }
+
+__global__ void __launch_bounds__(kColThreads) k_column(const Inst *__restrict__ insts, const Work *__restrict__ work,
+                                                        int kRK)
+{
+    extern __shared__ double2 ring_mem[];
     const Work w = work[blockIdx.x];
     const Inst &I = insts[w.inst];
-    const int col = w.j * blockDim.x + threadIdx.x;
-    if (col >= I.nc) return;
+    const int lane = threadIdx.x;
+    const int col = w.j * kColThreads + lane;
+    if (col >= I.nc) return;  // whole-warp granularity except the last block; no block barriers below
     const int nc = I.nc, nxh = I.nxh, nyu = I.nyu, nyv = I.nyv;
     const int i = col % nxh, kr = col / nxh;
     const RK rk = rk_coeffs(kRK);
@@ -72,35 +107,72 @@ __global__ void __launch_bounds__(128) k_column(const Inst *__restrict__ insts, 
     const double *du = I.dyu2i, *dv = I.dyv2i;
 
     // ---------------- A: right-hand sides and forward elimination --------
+    Ring ra{ring_mem, kSlotsA, lane};
+    auto fillA = [&](int j) {  // inputs of row j (1..nyu)
+        const int st = (j - 1) % kStages;
+        const size_t o = (size_t)j * nc, on = o - nc;
+        cp16(ra.at(st, 0), U1 + o + nc);
+        cp16(ra.at(st, 1), U3 + o + nc);
+        cp16(ra.at(st, 4), N1 + on);
+        cp16(ra.at(st, 5), N3 + on);
+        cp16(ra.at(st, 7), X1 + on);
+        cp16(ra.at(st, 8), X3 + on);
+        cp16(ra.at(st, 10), UVF + o);
+        cp16(ra.at(st, 11), WVF + o);
+        if (j <= nyv) {
+            cp16(ra.at(st, 2), U2 + o + nc);
+            cp16(ra.at(st, 3), P + o);  // p(j+1)
+            cp16(ra.at(st, 6), N2 + on);
+            cp16(ra.at(st, 9), X2 + on);
+            cp16(ra.at(st, 12), VVC + o + nc);
+        }
+    };
     // row 0: rhs = 0 and a = [0, 1, gw1] (u, w) / [0, 1, 0] (v)
     double2 u1m = U1[0], u1c = U1[(size_t)nc], u3m = U3[0], u3c = U3[(size_t)nc];
     double2 u2m = U2[0], u2c = U2[(size_t)nc];
+    double2 uvf_prev = UVF[0], wvf_prev = WVF[0];
+    double2 vvc_c = VVC[(size_t)nc];
+    double2 p_c = P[0];  // p(1)
     double a3u = I.gw1 * 1.0;
     double a3v = 0.0 * 1.0;
     double2 y1p = make_double2(0.0, 0.0), y3p = y1p, y2p = y1p;
+    for (int r = 0; r < kStages - 1; r++) {
+        if (1 + r <= nyu) fillA(1 + r);
+        cp_commit();
+    }
     U1[0] = y1p;
     U3[0] = y3p;
     U2[0] = y2p;
     FU[0] = a3u;
     FV[0] = a3v;
-    double2 uvf_prev = UVF[0], wvf_prev = WVF[0];
-    double2 vvc_c = VVC[(size_t)nc];
-    double2 p_c = P[0];  // p(1)
     for (int j = 1; j <= nyu; j++) {
-        const size_t o = (size_t)j * nc;  // row j of the u/v arrays
-        const size_t on = o - nc;         // row j of Nu/NXZ/P (stored from 1)
-        const double2 u1p = U1[o + nc], u3p = U3[o + nc];
+        cp_wait<kStages - 2>();
+        const int st = (j - 1) % kStages;
+        const size_t o = (size_t)j * nc;
+        const size_t on = o - nc;
+        const double2 u1p = *ra.at(st, 0), u3p = *ra.at(st, 1);
+        const double2 n1o = *ra.at(st, 4), n3o = *ra.at(st, 5);
+        const double2 x1 = *ra.at(st, 7), x3 = *ra.at(st, 8);
+        const double2 uvf = *ra.at(st, 10), wvf = *ra.at(st, 11);
+        double2 u2p, p_n, n2o, x2, vvn;
+        if (j <= nyv) {
+            u2p = *ra.at(st, 2);
+            p_n = *ra.at(st, 3);
+            n2o = *ra.at(st, 6);
+            x2 = *ra.at(st, 9);
+            vvn = *ra.at(st, 12);
+        }
+        if (j + kStages - 1 <= nyu) fillA(j + kStages - 1);
+        cp_commit();
+
         const double d1 = du[3 * j], d2 = du[3 * j + 1], d3 = du[3 * j + 2];
         const double cen = k2x + k2z + d2;
         double2 L1 = make_double2(d1 * u1m.x + cen * u1c.x + d3 * u1p.x, d1 * u1m.y + cen * u1c.y + d3 * u1p.y);
         double2 L3 = make_double2(d1 * u3m.x + cen * u3c.x + d3 * u3p.x, d1 * u3m.y + cen * u3c.y + d3 * u3p.y);
-        const double2 n1o = N1[on], n3o = N3[on];
         double2 du1 = make_double2(C1 * L1.x + C2 * n1o.x + dC3x * p_c.y, C1 * L1.y + C2 * n1o.y + -(dC3x * p_c.x));
         double2 du3 = make_double2(C1 * L3.x + C2 * n3o.x + dC3z * p_c.y, C1 * L3.y + C2 * n3o.y + -(dC3z * p_c.x));
         if (mean) du1.x = du1.x + C1m;
-        const double2 uvf = UVF[o], wvf = WVF[o];
         const double m = I.dthdyu[j];
-        const double2 x1 = X1[on], x3 = X3[on];
         const double2 nu1 = make_double2(x1.x + (uvf.x - uvf_prev.x) * m * ddv, x1.y + (uvf.y - uvf_prev.y) * m * ddv);
         const double2 nu3 = make_double2(x3.x + (wvf.x - wvf_prev.x) * m * ddv, x3.y + (wvf.y - wvf_prev.y) * m * ddv);
         N1[on] = nu1;
@@ -128,18 +200,13 @@ __global__ void __launch_bounds__(128) k_column(const Inst *__restrict__ insts, 
         uvf_prev = uvf;
         wvf_prev = wvf;
         if (j <= nyv) {
-            const double2 p_n = P[o];  // p(j+1)
-            const double2 u2p = U2[o + nc];
             const double e1 = dv[3 * j], e2 = dv[3 * j + 1], e3 = dv[3 * j + 2];
             const double cenv = k2x + k2z + e2;
             const double2 L2 = make_double2(e1 * u2m.x + cenv * u2c.x + e3 * u2p.x, e1 * u2m.y + cenv * u2c.y + e3 * u2p.y);
             const double mv = I.dthdyv[j];
             const double C3 = -rk.d * ddv * mv;
-            const double2 n2o = N2[on];
             double2 du2 = make_double2(C1 * L2.x + C2 * n2o.x + C3 * (p_n.x - p_c.x),
                                        C1 * L2.y + C2 * n2o.y + C3 * (p_n.y - p_c.y));
-            const double2 vvn = VVC[o + nc];
-            const double2 x2 = X2[on];
             const double2 nu2 = make_double2(x2.x + (vvn.x - vvc_c.x) * mv * ddv, x2.y + (vvn.y - vvc_c.y) * mv * ddv);
             N2[on] = nu2;
             du2 = make_double2(du2.x + G * nu2.x, du2.y + G * nu2.y);
@@ -159,6 +226,7 @@ __global__ void __launch_bounds__(128) k_column(const Inst *__restrict__ insts, 
             p_c = p_n;
         }
     }
+    cp_wait<0>();
     // top rows, rhs = 0: u/w a = [gw2, 1, 0], v a = [0, 1, 0]
     {
         const double inv = 1.0 / (1.0 - I.gw2 * a3u);
@@ -173,24 +241,47 @@ __global__ void __launch_bounds__(128) k_column(const Inst *__restrict__ insts, 
         U2[(size_t)(nyv + 1) * nc] = y2;
         y2p = y2;
     }
+    __threadfence_block();
 
     // ---------------- B: back substitution and divergence ---------------
     const double dtirk = (1.0 / dt) / (rk.a + rk.b);
     const bool div_inline = I.flag_ctpress != 0;
+    Ring rb{ring_mem, kSlotsB, lane};
+    auto fillB = [&](int j) {  // row j (nyu .. 0)
+        const int st = (nyu - j) % kStages;
+        const size_t o = (size_t)j * nc;
+        cp16(rb.at(st, 0), U1 + o);
+        cp16(rb.at(st, 1), U3 + o);
+        cp8(&rb.at(st, 3)->x, FU + o);
+        if (j <= nyv) {
+            cp16(rb.at(st, 2), U2 + o);
+            cp8(&rb.at(st, 3)->y, FV + o);
+        }
+    };
+    for (int r = 0; r < kStages - 1; r++) {
+        if (nyu - r >= 0) fillB(nyu - r);
+        cp_commit();
+    }
     double2 v1 = y1p, v3 = y3p;  // rows j+1 of u1, u3
     double2 v2 = y2p;            // u2 at row nyv+1 = nyu
     for (int j = nyu; j >= 0; j--) {
+        cp_wait<kStages - 2>();
+        const int st = (nyu - j) % kStages;
         const size_t o = (size_t)j * nc;
-        const double f = FU[o];
-        const double2 y1 = U1[o], y3 = U3[o];
+        const double2 y1 = *rb.at(st, 0), y3 = *rb.at(st, 1);
+        const double2 ff = *rb.at(st, 3);
+        double2 y2 = make_double2(0.0, 0.0);
+        if (j <= nyv) y2 = *rb.at(st, 2);
+        if (j - (kStages - 1) >= 0) fillB(j - (kStages - 1));
+        cp_commit();
+        const double f = ff.x;
         const double2 n1 = make_double2(y1.x - f * v1.x, y1.y - f * v1.y);
         const double2 n3 = make_double2(y3.x - f * v3.x, y3.y - f * v3.y);
         U1[o] = n1;
         U3[o] = n3;
         double2 n2 = v2;
         if (j <= nyv) {
-            const double fv = FV[o];
-            const double2 y2 = U2[o];
+            const double fv = ff.y;
             n2 = make_double2(y2.x - fv * v2.x, y2.y - fv * v2.y);
             U2[o] = n2;
         }
@@ -208,8 +299,10 @@ __global__ void __launch_bounds__(128) k_column(const Inst *__restrict__ insts, 
         v3 = n3;
         v2 = n2;
     }
+    cp_wait<0>();
 
     if (!div_inline) {
+        __threadfence_block();
         if (mean) {
             // flowrate_corr (littleharsh.f90:515-548): u11 from LUsol0 with
             // LU_build0 (tridLU_3D.f90:299-325); flowrateRe's dummy
@@ -222,20 +315,20 @@ __global__ void __launch_bounds__(128) k_column(const Inst *__restrict__ insts, 
             u11[0] = yp;
             f11[0] = a3p;
             for (int j = 1; j <= ne; j++) {
-                double a1, a2, a3, r;
+                double a1, a2, a3, rr;
                 if (j < ne) {
                     a1 = -beta * du[3 * j];
                     a2 = 1.0 - beta * du[3 * j + 1];
                     a3 = -beta * du[3 * j + 2];
-                    r = bdt;
+                    rr = bdt;
                 } else {
                     a1 = I.gw2;
                     a2 = 1.0;
                     a3 = 0.0;
-                    r = 0.0;
+                    rr = 0.0;
                 }
                 const double inv = 1.0 / (a2 - a1 * a3p);
-                yp = (r - a1 * yp) * inv;
+                yp = (rr - a1 * yp) * inv;
                 a3p = a3 * inv;
                 u11[j] = yp;
                 f11[j] = a3p;
@@ -270,38 +363,74 @@ __global__ void __launch_bounds__(128) k_column(const Inst *__restrict__ insts, 
             v2m = v2c;
         }
     }
+    __threadfence_block();
 
     // ---------------- C: LUsolP forward sweep ------------------------------
     const double *G2 = I.DG2 + col, *G3 = I.DG3 + col;
+    Ring rc{ring_mem, kSlotsC, lane};
+    auto fillC = [&](int j) {  // row j (2 .. nyu)
+        const int st = (j - 2) % kStages;
+        const size_t o = (size_t)(j - 1) * nc;
+        cp16(rc.at(st, 0), PS + o);
+        cp8(&rc.at(st, 1)->x, G2 + o);
+    };
+    for (int r = 0; r < kStages - 1; r++) {
+        if (2 + r <= nyu) fillC(2 + r);
+        cp_commit();
+    }
     double2 xp = cscale(G2[0], PS[0]);
     PS[0] = xp;
     for (int j = 2; j <= nyu; j++) {
-        const size_t o = (size_t)(j - 1) * nc;
+        cp_wait<kStages - 2>();
+        const int st = (j - 2) % kStages;
+        const double2 x = *rc.at(st, 0);
+        const double g2 = rc.at(st, 1)->x;
+        if (j + kStages - 1 <= nyu) fillC(j + kStages - 1);
+        cp_commit();
         const double g1 = I.DG1[j];
-        const double2 x = PS[o];
-        xp = make_double2((x.x - g1 * xp.x) * G2[o], (x.y - g1 * xp.y) * G2[o]);
-        PS[o] = xp;
+        xp = make_double2((x.x - g1 * xp.x) * g2, (x.y - g1 * xp.y) * g2);
+        PS[(size_t)(j - 1) * nc] = xp;
     }
+    cp_wait<0>();
+    __threadfence_block();
 
     // ---------------- D: LUsolP back sweep, p += psi, v_corr --------------
     const double dtrk = dt * (rk.a + rk.b);
     const double kxd = dtrk * kxr, kzd = dtrk * kzr;
     const double dtrk_u2 = dtrk * ddv;
-    double2 psn = xp;  // psi(j+1); at j = nyu psi(nyu) = x(nyu)
+    Ring rd{ring_mem, kSlotsD, lane};
+    auto fillD = [&](int j) {  // row j (nyu .. 1)
+        const int st = (nyu - j) % kStages;
+        const size_t o = (size_t)(j - 1) * nc, ou = (size_t)j * nc;
+        cp16(rd.at(st, 0), PS + o);
+        cp16(rd.at(st, 1), P + o);
+        cp16(rd.at(st, 2), U1 + ou);
+        cp16(rd.at(st, 3), U3 + ou);
+        if (j <= nyv) cp16(rd.at(st, 4), U2 + ou);
+        if (j < nyu) cp8(&rd.at(st, 5)->x, G3 + o);
+    };
+    for (int r = 0; r < kStages - 1; r++) {
+        if (nyu - r >= 1) fillD(nyu - r);
+        cp_commit();
+    }
+    double2 psn = make_double2(0.0, 0.0);  // psi(j+1)
     bool bad = false;
     for (int j = nyu; j >= 1; j--) {
+        cp_wait<kStages - 2>();
+        const int st = (nyu - j) % kStages;
+        const double2 x = *rd.at(st, 0), p = *rd.at(st, 1);
+        double2 a = *rd.at(st, 2), c3 = *rd.at(st, 3);
+        double2 v = make_double2(0.0, 0.0);
+        if (j <= nyv) v = *rd.at(st, 4);
+        const double g3 = rd.at(st, 5)->x;
+        if (j - (kStages - 1) >= 1) fillD(j - (kStages - 1));
+        cp_commit();
         const size_t o = (size_t)(j - 1) * nc;
-        double2 ps = psn;
-        if (j < nyu) {
-            const double2 x = PS[o];
-            const double g3 = G3[o];
-            ps = make_double2(x.x - g3 * psn.x, x.y - g3 * psn.y);
-        }
+        double2 ps = x;  // psi(nyu) = x(nyu)
+        if (j < nyu) ps = make_double2(x.x - g3 * psn.x, x.y - g3 * psn.y);
         PS[o] = ps;
-        const double2 p = P[o];
         P[o] = make_double2(p.x + ps.x, p.y + ps.y);
         const size_t ou = (size_t)j * nc;
-        double2 a = U1[ou], c3 = U3[ou];
         a = make_double2(a.x - -(kxd * ps.y), a.y - kxd * ps.x);
         c3 = make_double2(c3.x - -(kzd * ps.y), c3.y - kzd * ps.x);
         U1[ou] = a;
@@ -316,18 +445,19 @@ __global__ void __launch_bounds__(128) k_column(const Inst *__restrict__ insts, 
             bad = !isfinite(a.x) || !isfinite(a.y) || !isfinite(ps.x) || !isfinite(ps.y);
         }
         if (j <= nyv) {
-            double2 v = U2[ou];
             const double mv = dtrk_u2 * I.dthdyv[j];
             v = make_double2(v.x - mv * (psn.x - ps.x), v.y - mv * (psn.y - ps.y));
             U2[ou] = v;
         }
         psn = ps;
     }
+    cp_wait<0>();
     U2[0] = make_double2(0.0, 0.0);
     U2[(size_t)(nyv + 1) * nc] = make_double2(0.0, 0.0);
     if (bad) atomicOr(I.err, ERR_NONFINITE);
     if (mean && kRK == 3) {
         // flowrateIm (littleharsh.f90:473-492) via meanflow_ctP (:572-589)
+        __threadfence_block();
         double Qu = 0.0;
         for (int j = 1; j <= nyv + 1; j++) Qu = Qu + (I.yv[j] - I.yv[j - 1]) * U1[(size_t)j * nc].x;
         I.sc[SC_QX] = Qu;

@@ -3,6 +3,8 @@
 #include "lh_engine.h"
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "lh_kernels.cuh"
@@ -231,46 +233,143 @@ cudaError_t instance_download(DevInstance &d, double *u1, double *u2, double *u3
 }
 
 // ---------------------------------------------------------------------------
-cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, const Tiles &t)
+namespace {
+struct ClassTiles {
+    bool fast;
+    int cbz, rbx, cbf;
+    int tz, tx, tf;
+    size_t smz, smx, smf;
+};
+
+ClassTiles fast_tiles(const HostSetup &s, int cbz_max, int rb, int cbf_max)
+{
+    ClassTiles c{};
+    c.fast = true;
+    int nb = (s.nxh + cbz_max - 1) / cbz_max;
+    c.cbz = (s.nxh + nb - 1) / nb;
+    c.tz = fast_threads(s.Mz, c.cbz);
+    c.smz = (size_t)s.Mz * (1 + c.cbz) * sizeof(double2);
+    c.rbx = rb;
+    c.tx = fast_threads(s.Mx, 3 * rb);
+    c.smx = (size_t)s.Mx * (1 + 3 * rb) * sizeof(double2);
+    nb = (s.nxh + cbf_max - 1) / cbf_max;
+    c.cbf = (s.nxh + nb - 1) / nb;
+    c.tf = fast_threads(s.Mz, 6 * c.cbf);
+    c.smf = (size_t)s.Mz * (1 + 6 * c.cbf) * sizeof(double2);
+    return c;
+}
+
+ClassTiles class_tiles(const HostSetup &s, bool force_generic)
+{
+    ClassTiles c{};
+    c.fast = !force_generic && fast_size(s.Mz) && fast_size(s.Mx);
+    const char *ov = getenv("LH_TILES");
+    int a = 0, b = 0, d = 0;
+    if (c.fast && ov && sscanf(ov, "%d,%d,%d", &a, &b, &d) == 3 && a > 0 && b > 0 && d > 0) return fast_tiles(s, a, b, d);
+    if (c.fast) {
+        const int mz = fast_threads(s.Mz, 1), mx = fast_threads(s.Mx, 1);  // max(N1,N2) rounded to 32
+        (void)mz;
+        (void)mx;
+        // z inverse: up to 16 x modes per CTA, balanced blocks
+        int nb = (s.nxh + 15) / 16;
+        c.cbz = (s.nxh + nb - 1) / nb;
+        c.tz = fast_threads(s.Mz, c.cbz);
+        c.smz = (size_t)s.Mz * (1 + c.cbz) * sizeof(double2);
+        // x products: 3 rb vectors, <= 512 threads, <= 110 KB
+        int rb = 8;
+        while (rb > 1 && (fast_threads(s.Mx, 3 * rb) > 512 || (size_t)s.Mx * (1 + 3 * rb) * 16 > 110 * 1024)) rb--;
+        c.rbx = rb;
+        c.tx = fast_threads(s.Mx, 3 * rb);
+        c.smx = (size_t)s.Mx * (1 + 3 * rb) * sizeof(double2);
+        // z forward: 6 cb vectors, <= 512 threads, <= 110 KB
+        int cbmax = 8;
+        while (cbmax > 1 && (fast_threads(s.Mz, 6 * cbmax) > 512 || (size_t)s.Mz * (1 + 6 * cbmax) * 16 > 110 * 1024))
+            cbmax--;
+        nb = (s.nxh + cbmax - 1) / cbmax;
+        c.cbf = (s.nxh + nb - 1) / nb;
+        c.tf = fast_threads(s.Mz, 6 * c.cbf);
+        c.smf = (size_t)s.Mz * (1 + 6 * c.cbf) * sizeof(double2);
+    } else {
+        Tiles t = default_tiles(s.Mx, s.Mz, s.nxh, s.nyu);
+        c.cbz = t.bc_zinv;
+        c.rbx = t.br_x;
+        c.cbf = t.bc_zfwd;
+        c.tz = c.tx = c.tf = t.threads;
+        c.smz = smem_zinv(t, s.Mz);
+        c.smx = smem_x(t, s.Mx);
+        c.smf = smem_zfwd(t, s.Mz);
+    }
+    return c;
+}
+}  // namespace
+
+cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, bool force_generic)
 {
     plan_free(p);
-    p.tiles = t;
+    p.force_generic = force_generic;
     p.ninst = (int)insts.size();
+    // size classes in order of first appearance
+    std::vector<std::pair<int, int>> classes;
+    std::vector<int> cls_of(insts.size());
     int rounds = 0;
-    int maxMx = 0, maxMz = 0;
-    for (auto *d : insts) {
-        rounds = std::max(rounds, (d->hs.nyu + d->inst.chunk - 1) / d->inst.chunk);
-        maxMx = std::max(maxMx, d->hs.Mx);
-        maxMz = std::max(maxMz, d->hs.Mz);
+    for (size_t q = 0; q < insts.size(); q++) {
+        const HostSetup &s = insts[q]->hs;
+        std::pair<int, int> key(s.Mz, s.Mx);
+        auto it = std::find(classes.begin(), classes.end(), key);
+        if (it == classes.end()) {
+            classes.push_back(key);
+            it = classes.end() - 1;
+        }
+        cls_of[q] = (int)(it - classes.begin());
+        rounds = std::max(rounds, (s.nyu + insts[q]->inst.chunk - 1) / insts[q]->inst.chunk);
     }
-    p.zinv.assign(rounds, {});
-    p.xprod.assign(rounds, {});
-    p.zfwd.assign(rounds, {});
+    const size_t ncls = classes.size();
+    std::vector<ClassTiles> tiles(ncls);
+    std::vector<const HostSetup *> rep(ncls, nullptr);
+    for (size_t q = 0; q < insts.size(); q++)
+        if (!rep[cls_of[q]]) rep[cls_of[q]] = &insts[q]->hs;
+    for (size_t c = 0; c < ncls; c++) tiles[c] = class_tiles(*rep[c], force_generic);
+    // work lists [round][stage][class]
+    std::vector<std::vector<std::vector<std::vector<Work>>>> lists(
+        rounds, std::vector<std::vector<std::vector<Work>>>(3, std::vector<std::vector<Work>>(ncls)));
     p.column.clear();
     for (int q = 0; q < (int)insts.size(); q++) {
         const HostSetup &s = insts[q]->hs;
+        const ClassTiles &ct = tiles[cls_of[q]];
         const int chunk = insts[q]->inst.chunk;
-        const int nbz = (s.nxh + t.bc_zinv - 1) / t.bc_zinv;
-        const int nbx = (s.Mz + t.br_x - 1) / t.br_x;
-        const int nbf = (s.nxh + t.bc_zfwd - 1) / t.bc_zfwd;
+        const int nbz = (s.nxh + ct.cbz - 1) / ct.cbz;
+        const int nbx = (s.Mz + ct.rbx - 1) / ct.rbx;
+        const int nbf = (s.nxh + ct.cbf - 1) / ct.cbf;
         for (int j = 1; j <= s.nyu; j++) {
             const int r = (j - 1) / chunk, slot = (j - 1) % chunk;
+            auto &L = lists[r];
             for (int f = 0; f < kNumProducts; f++)
-                for (int b = 0; b < nbz; b++) p.zinv[r].push_back({q, j, slot, f * nbz + b});
-            for (int b = 0; b < nbx; b++) p.xprod[r].push_back({q, j, slot, b});
-            for (int b = 0; b < nbf; b++) p.zfwd[r].push_back({q, j, slot, b});
+                for (int b = 0; b < nbz; b++) L[0][cls_of[q]].push_back({q, j, slot, f * nbz + b});
+            for (int b = 0; b < nbx; b++) L[1][cls_of[q]].push_back({q, j, slot, b});
+            for (int b = 0; b < nbf; b++) L[2][cls_of[q]].push_back({q, j, slot, b});
         }
-        for (int b = 0; b < (s.nc + 127) / 128; b++) p.column.push_back({q, b, 0, 0});
+        for (int b = 0; b < (s.nc + kColumnThreads - 1) / kColumnThreads; b++) p.column.push_back({q, b, 0, 0});
     }
     std::vector<Work> all;
-    for (int r = 0; r < rounds; r++) {
-        p.off_zinv.push_back(all.size());
-        all.insert(all.end(), p.zinv[r].begin(), p.zinv[r].end());
-        p.off_xprod.push_back(all.size());
-        all.insert(all.end(), p.xprod[r].begin(), p.xprod[r].end());
-        p.off_zfwd.push_back(all.size());
-        all.insert(all.end(), p.zfwd[r].begin(), p.zfwd[r].end());
-    }
+    p.rounds.assign(rounds, {});
+    for (int r = 0; r < rounds; r++)
+        for (int stg = 0; stg < 3; stg++)
+            for (size_t c = 0; c < ncls; c++) {
+                const auto &v = lists[r][stg][c];
+                if (v.empty()) continue;
+                Group g;
+                g.stage = stg;
+                g.fast = tiles[c].fast;
+                g.Mz = classes[c].first;
+                g.Mx = classes[c].second;
+                g.off = all.size();
+                g.count = v.size();
+                g.threads = stg == 0 ? tiles[c].tz : stg == 1 ? tiles[c].tx : tiles[c].tf;
+                g.smem = stg == 0 ? tiles[c].smz : stg == 1 ? tiles[c].smx : tiles[c].smf;
+                g.param = stg == 0 ? tiles[c].cbz : stg == 1 ? tiles[c].rbx : tiles[c].cbf;
+                all.insert(all.end(), v.begin(), v.end());
+                p.rounds[r].push_back(g);
+            }
     p.off_column = all.size();
     all.insert(all.end(), p.column.begin(), p.column.end());
     cudaError_t e = cudaMalloc(&p.d_work, all.size() * sizeof(Work));
@@ -280,42 +379,82 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, c
     }
     e = cudaMemcpy(p.d_work, all.data(), all.size() * sizeof(Work), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return e;
-    p.sm_zinv = smem_zinv(t, maxMz);
-    p.sm_x = smem_x(t, maxMx);
-    p.sm_zfwd = smem_zfwd(t, maxMz);
-    if ((e = cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.sm_zinv)) !=
-        cudaSuccess)
+    // dynamic shared-memory limits for every kernel this plan launches
+    size_t gz = 0, gx = 0, gf = 0;
+    for (size_t c = 0; c < ncls; c++) {
+        if (tiles[c].fast) {
+            if ((e = fast_set_attributes(classes[c].first, classes[c].second, tiles[c].smz, tiles[c].smx,
+                                         tiles[c].smf)) != cudaSuccess)
+                return e;
+        } else {
+            gz = std::max(gz, tiles[c].smz);
+            gx = std::max(gx, tiles[c].smx);
+            gf = std::max(gf, tiles[c].smf);
+        }
+    }
+    if (gz && (e = cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gz)) != cudaSuccess)
         return e;
-    if ((e = cudaFuncSetAttribute(k_xprod, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.sm_x)) != cudaSuccess)
+    if (gx && (e = cudaFuncSetAttribute(k_xprod, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gx)) != cudaSuccess)
         return e;
-    if ((e = cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.sm_zfwd)) !=
-        cudaSuccess)
+    if (gf && (e = cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gf)) != cudaSuccess)
         return e;
-    return cudaSuccess;
+    p.sm_col = column_smem_bytes();
+    return cudaFuncSetAttribute(k_column, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.sm_col);
 }
 
 void plan_free(Plan &p)
 {
     if (p.d_work) cudaFree(p.d_work);
     p.d_work = nullptr;
-    p.off_zinv.clear();
-    p.off_xprod.clear();
-    p.off_zfwd.clear();
+    p.rounds.clear();
 }
 
-cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl_any, cudaStream_t st)
+static void time_begin(LaunchTimer *t, cudaStream_t st)
 {
-    const Tiles &t = p.tiles;
-    for (size_t r = 0; r < p.zinv.size(); r++) {
-        k_zinv<<<(unsigned)p.zinv[r].size(), t.threads, p.sm_zinv, st>>>(d_insts, p.d_work + p.off_zinv[r],
-                                                                         t.bc_zinv);
-        k_xprod<<<(unsigned)p.xprod[r].size(), t.threads, p.sm_x, st>>>(d_insts, p.d_work + p.off_xprod[r], t.br_x,
-                                                                        (kRK == 1 && cfl_any) ? 1 : 0);
-        k_zfwd<<<(unsigned)p.zfwd[r].size(), t.threads, p.sm_zfwd, st>>>(d_insts, p.d_work + p.off_zfwd[r],
-                                                                         t.bc_zfwd);
+    if (t) cudaEventRecord(t->ev[0], st);
+}
+
+static cudaError_t time_end(LaunchTimer *t, int cls, cudaStream_t st)
+{
+    if (!t) return cudaSuccess;
+    cudaEventRecord(t->ev[1], st);
+    cudaError_t e = cudaEventSynchronize(t->ev[1]);
+    float f = 0.f;
+    cudaEventElapsedTime(&f, t->ev[0], t->ev[1]);
+    t->ms[cls] += f;
+    t->n[cls] += 1;
+    return e;
+}
+
+cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl_any, cudaStream_t st,
+                           LaunchTimer *timer)
+{
+    const int want_max = (kRK == 1 && cfl_any) ? 1 : 0;
+    cudaError_t e = cudaSuccess;
+    for (const auto &round : p.rounds)
+        for (const Group &g : round) {
+            const Work *w = p.d_work + g.off;
+            const unsigned n = (unsigned)g.count;
+            time_begin(timer, st);
+            if (g.fast) {
+                if (g.stage == 0) fast_launch_zinv(g.Mz, n, g.threads, g.smem, st, d_insts, w, g.param);
+                else if (g.stage == 1) fast_launch_xprod(g.Mx, n, g.threads, g.smem, st, d_insts, w, g.param, want_max);
+                else fast_launch_zfwd(g.Mz, n, g.threads, g.smem, st, d_insts, w, g.param);
+            } else {
+                if (g.stage == 0) k_zinv<<<n, g.threads, g.smem, st>>>(d_insts, w, g.param);
+                else if (g.stage == 1) k_xprod<<<n, g.threads, g.smem, st>>>(d_insts, w, g.param, want_max);
+                else k_zfwd<<<n, g.threads, g.smem, st>>>(d_insts, w, g.param);
+            }
+            if ((e = time_end(timer, g.stage, st)) != cudaSuccess) return e;
+        }
+    if (kRK == 1) {
+        time_begin(timer, st);
+        k_dt<<<p.ninst, 256, 0, st>>>(d_insts, p.ninst);
+        if ((e = time_end(timer, 3, st)) != cudaSuccess) return e;
     }
-    if (kRK == 1) k_dt<<<p.ninst, 256, 0, st>>>(d_insts, p.ninst);
-    k_column<<<(unsigned)p.column.size(), 128, 0, st>>>(d_insts, p.d_work + p.off_column, kRK);
+    time_begin(timer, st);
+    k_column<<<(unsigned)p.column.size(), kColumnThreads, p.sm_col, st>>>(d_insts, p.d_work + p.off_column, kRK);
+    if ((e = time_end(timer, 4, st)) != cudaSuccess) return e;
     return cudaGetLastError();
 }
 

@@ -48,21 +48,41 @@ cudaError_t instance_upload(DevInstance &d, const double *u1, const double *u2, 
 cudaError_t instance_download(DevInstance &d, double *u1, double *u2, double *u3, double *p, cudaStream_t st);
 cudaError_t download_field(const DevInstance &d, const double2 *src, int len, double *dst, cudaStream_t st);
 
-// Work tables for a set of instances sharing launches.
-struct Plan {
-    std::vector<std::vector<Work>> zinv, xprod, zfwd;  // per chunk round
-    std::vector<Work> column;
-    Work *d_work = nullptr;  // all tables back to back
-    std::vector<size_t> off_zinv, off_xprod, off_zfwd;
-    size_t off_column = 0;
-    Tiles tiles;
-    size_t sm_zinv = 0, sm_x = 0, sm_zfwd = 0;
-    int ninst = 0;
+// One kernel launch of the plane pipeline: all work items of one stage for
+// the instances of one size class in one chunk round.
+struct Group {
+    int stage = 0;        // 0 z inverse, 1 x products, 2 z forward
+    bool fast = false;    // compile-time-sized kernels
+    int Mz = 0, Mx = 0;
+    size_t off = 0, count = 0;
+    int threads = 256;
+    size_t smem = 0;
+    int param = 1;        // cb (z stages) or rb (x stage)
 };
 
-cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, const Tiles &t);
+// Work tables for a set of instances sharing launches.
+struct Plan {
+    std::vector<std::vector<Group>> rounds;  // launch order within a round
+    std::vector<Work> column;
+    Work *d_work = nullptr;  // all tables back to back
+    size_t off_column = 0;
+    size_t sm_col = 0;
+    int ninst = 0;
+    bool force_generic = false;
+};
+
+// Optional per-launch timing (kernel classes 0 z inverse, 1 x products,
+// 2 z forward, 3 dt, 4 column).
+struct LaunchTimer {
+    cudaEvent_t ev[2];
+    double ms[5] = {0, 0, 0, 0, 0};
+    int n[5] = {0, 0, 0, 0, 0};
+};
+
+cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, bool force_generic = false);
 void plan_free(Plan &p);
 // Enqueue one substep of every instance of the plan.
-cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl_any, cudaStream_t st);
+cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl_any, cudaStream_t st,
+                           LaunchTimer *timer = nullptr);
 
 }  // namespace lh

@@ -5,6 +5,9 @@
 
 namespace lh {
 
+constexpr int kColumnThreads = 32;  // one warp of columns per column-pass CTA
+size_t column_smem_bytes();
+
 __global__ void k_zinv(const Inst *__restrict__ insts, const Work *__restrict__ work, int bc);
 __global__ void k_xprod(const Inst *__restrict__ insts, const Work *__restrict__ work, int br, int want_max);
 __global__ void k_zfwd(const Inst *__restrict__ insts, const Work *__restrict__ work, int bc);
@@ -22,5 +25,16 @@ __global__ void k_lusolu(const Inst *__restrict__ insts, int grid, int kRK, doub
                          double2 *u, double *fac);
 __global__ void k_lusolp(const Inst *__restrict__ insts, double2 *x);
 __global__ void k_divmax(const Inst *__restrict__ insts, double *out);
+
+// compile-time-sized fast path (lh_plane_fast.cu)
+bool fast_size(int n);
+int fast_threads(int n, int vectors);
+cudaError_t fast_set_attributes(int Mz, int Mx, size_t smz, size_t smx, size_t smf);
+void fast_launch_zinv(int Mz, unsigned grid, int threads, size_t smem, cudaStream_t st, const Inst *insts,
+                      const Work *work, int cb);
+void fast_launch_xprod(int Mx, unsigned grid, int threads, size_t smem, cudaStream_t st, const Inst *insts,
+                       const Work *work, int rb, int want_max);
+void fast_launch_zfwd(int Mz, unsigned grid, int threads, size_t smem, cudaStream_t st, const Inst *insts,
+                      const Work *work, int cb);
 
 }  // namespace lh
