@@ -15,16 +15,7 @@
 
 using namespace lh;
 
-struct lh_ctx {
-    DevInstance dev;
-    Plan plan;
-    Inst *d_inst = nullptr;
-    cudaStream_t st = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-    bool have_state = false;
-    std::string err;
-};
+#include "lh_ctx_internal.h"
 
 static int fail(lh_ctx *c, int code, const std::string &msg)
 {

@@ -1,0 +1,19 @@
+// Definition of the single-instance context shared by the C-ABI sources.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "lh_engine.h"
+
+struct lh_ctx {
+    lh::DevInstance dev;
+    lh::Plan plan;
+    lh::Inst *d_inst = nullptr;
+    cudaStream_t st = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    bool have_state = false;
+    std::string err;
+};

@@ -1,0 +1,166 @@
+! iso_c_binding bridge from the LittleHarsh Fortran driver to the B200
+! engine (include/lh_gpu.h).  The Fortran main loop keeps its arrays and
+! its set-up; these wrappers forward them to the C ABI with the reference's
+! own subroutine names and argument lists, so littleharsh.f90 and FOU3D.f90
+! call sites stay as they are.  A non-zero status stops the run the way the
+! reference stops on bad input (start.f90:203-204).
+!
+! Build (Fortran compiler and the engine library required):
+!   mpif90 -c lh_gpu_bridge.f90
+!   mpif90 -o littleharsh <reference objects> lh_gpu_bridge.o \
+!          -L<repo>/final-single-block-_b200/build -llh_gpu -lcudart
+module lh_gpu_bridge
+  use iso_c_binding
+  implicit none
+
+  type, bind(C) :: lh_grid_desc
+    integer(c_int)  :: Nx, Nz, ny
+    real(c_double)  :: Re, alp, bet, mpgx
+    integer(c_int)  :: flag_ctpress, grid_type
+    real(c_double)  :: dyq
+    integer(c_int)  :: ppp
+    real(c_double)  :: gamma
+    integer(c_int)  :: dt_mode
+    real(c_double)  :: CFL, dt
+  end type lh_grid_desc
+
+  interface
+    integer(c_int) function lh_ctx_create(desc, ctx) bind(C, name="lh_ctx_create")
+      import :: c_int, c_ptr, lh_grid_desc
+      type(lh_grid_desc), intent(in) :: desc
+      type(c_ptr), intent(out)       :: ctx
+    end function
+    integer(c_int) function lh_ctx_destroy(ctx) bind(C, name="lh_ctx_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function lh_upload_state(ctx, u1, u2, u3, p) bind(C, name="lh_upload_state")
+      import :: c_int, c_ptr, c_double_complex
+      type(c_ptr), value :: ctx
+      complex(c_double_complex), intent(in) :: u1(*), u2(*), u3(*), p(*)
+    end function
+    integer(c_int) function lh_download_state(ctx, u1, u2, u3, p) bind(C, name="lh_download_state")
+      import :: c_int, c_ptr, c_double_complex
+      type(c_ptr), value :: ctx
+      complex(c_double_complex), intent(out) :: u1(*), u2(*), u3(*), p(*)
+    end function
+    integer(c_int) function lh_substep(ctx, kRK) bind(C, name="lh_substep")
+      import :: c_int, c_ptr
+      type(c_ptr), value    :: ctx
+      integer(c_int), value :: kRK
+    end function
+    integer(c_int) function lh_step(ctx, nsteps) bind(C, name="lh_step")
+      import :: c_int, c_ptr
+      type(c_ptr), value    :: ctx
+      integer(c_int), value :: nsteps
+    end function
+    integer(c_int) function lh_get_scalars(ctx, t, dt, iter, mpgx, qx) bind(C, name="lh_get_scalars")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(out) :: t, dt, mpgx, qx
+      integer(c_int), intent(out) :: iter
+    end function
+    integer(c_int) function lh_four_to_phys(ctx, planes, n) bind(C, name="lh_four_to_phys")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value    :: ctx
+      real(c_double)        :: planes(*)
+      integer(c_int), value :: n
+    end function
+    integer(c_int) function lh_phys_to_four(ctx, planes, n) bind(C, name="lh_phys_to_four")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value    :: ctx
+      real(c_double)        :: planes(*)
+      integer(c_int), value :: n
+    end function
+    integer(c_int) function lh_lusolu(ctx, grid, kRK, dt, rhs, u) bind(C, name="lh_lusolu")
+      import :: c_int, c_ptr, c_double, c_double_complex
+      type(c_ptr), value    :: ctx
+      integer(c_int), value :: grid, kRK
+      real(c_double), value :: dt
+      complex(c_double_complex), intent(in)  :: rhs(*)
+      complex(c_double_complex), intent(out) :: u(*)
+    end function
+    integer(c_int) function lh_lusolp(ctx, x) bind(C, name="lh_lusolp")
+      import :: c_int, c_ptr, c_double_complex
+      type(c_ptr), value :: ctx
+      complex(c_double_complex) :: x(*)
+    end function
+  end interface
+
+  type(c_ptr), save :: gpu_ctx = c_null_ptr
+
+contains
+
+  subroutine gpu_check(rc, where)
+    integer(c_int), intent(in) :: rc
+    character(*), intent(in)   :: where
+    if (rc /= 0) then
+      write(*,*) 'lh_gpu error', rc, 'in ', where
+      stop
+    end if
+  end subroutine
+
+  ! After start(): describe the instance from the declaration module.
+  subroutine gpu_start()
+    use declaration
+    type(lh_grid_desc) :: d
+    d%Nx = Nspec_x; d%Nz = Nspec_z; d%ny = nyv + 2
+    d%Re = Re; d%alp = alp; d%bet = bet; d%mpgx = mpgx
+    d%flag_ctpress = flag_ctpress
+    d%grid_type = 0; d%dyq = dyq; d%ppp = ppp; d%gamma = 0d0
+    d%dt_mode = 0; d%CFL = CFL; d%dt = 0d0
+    call gpu_check(lh_ctx_create(d, gpu_ctx), 'lh_ctx_create')
+  end subroutine
+
+  ! After getini(): hand the initial state to the device.
+  subroutine gpu_getini(u1, u2, u3, p)
+    complex(8), intent(in) :: u1(*), u2(*), u3(*), p(*)
+    call gpu_check(lh_upload_state(gpu_ctx, u1, u2, u3, p), 'lh_upload_state')
+  end subroutine
+
+  ! Replaces the body of the substep loop, littleharsh.f90:169-220
+  ! (RHS0_u1/2/3, nonlinear, solveU x3, meanflow_ctU, solveP, v_corr).
+  subroutine gpu_substep(kRK_in)
+    integer, intent(in) :: kRK_in
+    call gpu_check(lh_substep(gpu_ctx, int(kRK_in, c_int)), 'lh_substep')
+  end subroutine
+
+  ! Bring the state back for record_out / stats on output steps.
+  subroutine gpu_fetch(u1, u2, u3, p)
+    complex(8), intent(out) :: u1(*), u2(*), u3(*), p(*)
+    call gpu_check(lh_download_state(gpu_ctx, u1, u2, u3, p), 'lh_download_state')
+  end subroutine
+
+  ! four_to_phys_u / phys_to_four_du on one plane (FOU3D.f90:653, 1654)
+  subroutine gpu_four_to_phys_du(du)
+    real(8) :: du(*)
+    call gpu_check(lh_four_to_phys(gpu_ctx, du, 1_c_int), 'lh_four_to_phys')
+  end subroutine
+
+  subroutine gpu_phys_to_four_du(duPL)
+    real(8) :: duPL(*)
+    call gpu_check(lh_phys_to_four(gpu_ctx, duPL, 1_c_int), 'lh_phys_to_four')
+  end subroutine
+
+  ! LUsolU(u, rhsu, a, grid, myid) without the a(3,:) work array
+  ! (tridLU_3D.f90:38-94); uses the module's kRK and dt.
+  subroutine gpu_LUsolU(u, rhsu, grid)
+    use declaration, only: kRK, dt
+    complex(8), intent(out) :: u(*)
+    complex(8), intent(in)  :: rhsu(*)
+    integer, intent(in)     :: grid
+    call gpu_check(lh_lusolu(gpu_ctx, int(grid, c_int), int(kRK, c_int), dt, rhsu, u), 'lh_lusolu')
+  end subroutine
+
+  ! LUsolP(x, myid, nystart, nyend) with the DG factors of start()
+  subroutine gpu_LUsolP(x)
+    complex(8) :: x(*)
+    call gpu_check(lh_lusolp(gpu_ctx, x), 'lh_lusolp')
+  end subroutine
+
+  subroutine gpu_finalize()
+    if (c_associated(gpu_ctx)) call gpu_check(lh_ctx_destroy(gpu_ctx), 'lh_ctx_destroy')
+    gpu_ctx = c_null_ptr
+  end subroutine
+
+end module lh_gpu_bridge
