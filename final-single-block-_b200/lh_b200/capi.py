@@ -26,7 +26,7 @@ EXPORTS = [
     "lh_upload_state", "lh_download_state", "lh_download_nu", "lh_substep", "lh_step",
     "lh_get_scalars", "lh_step_host", "lh_synchronize", "lh_get_stream", "lh_profile",
     "lh_error_div", "lh_get_intermediate", "lh_four_to_phys", "lh_phys_to_four", "lh_lusolu",
-    "lh_lusolp", "lh_batch_create", "lh_batch_destroy", "lh_batch_last_error",
+    "lh_lusolp", "lh_lusolu_noalloc", "lh_batch_create", "lh_batch_destroy", "lh_batch_last_error",
     "lh_instance_bytes", "lh_batch_add", "lh_batch_remove", "lh_batch_step",
     "lh_batch_download", "lh_batch_scalars", "lh_batch_count", "lh_batch_synchronize",
 ]
@@ -129,6 +129,7 @@ def lib() -> ctypes.CDLL:
         "lh_phys_to_four": (i, [v, dp, i]),
         "lh_lusolu": (i, [v, i, i, d, dp, dp]),
         "lh_lusolp": (i, [v, dp]),
+        "lh_lusolu_noalloc": (i, [v, i, i, d, v, v]),
         "lh_batch_create": (i, [sz, P(v)]),
         "lh_batch_destroy": (i, [v]),
         "lh_batch_last_error": (ctypes.c_char_p, [v]),

@@ -137,6 +137,23 @@ int lh_lusolu(lh_ctx *ctx, int grid, int kRK, double dt, const double *rhs,
               double *u);
 int lh_lusolp(lh_ctx *ctx, double *x);
 
+/* Allocation-free LUsolU for callers that cannot allocate device memory
+ * per call (inside CUDA-graph capture, in a loop that must not hit the
+ * synchronisation of cudaMalloc/cudaFree, or with device memory owned by
+ * another allocator).  No counterpart in the reference.  rhs_dev and u_dev
+ * are device arrays the caller owns, in the engine's plane-major layout:
+ * complex element (j, column) at j*ncols + column, rows 0..nyu+1 (grid 2)
+ * or 0..nyv+1 (grid 1); they may be the same array.  The only scratch is a
+ * fixed file-scope device array of 2^21 doubles (16 MiB, held on every GPU
+ * that loads the library); rows x columns above that return LH_EINVAL.
+ * The first call on a device looks the array's device address up
+ * (cudaGetSymbolAddress), so make it before any stream capture.  Calls are
+ * ordered on the context's stream; calls that overlap on the GPU (other
+ * streams, other contexts on the same device) share the scratch and race.
+ * Every call overwrites the scratch rows it uses before reading them. */
+int lh_lusolu_noalloc(lh_ctx *ctx, int grid, int kRK, double dt,
+                      const double *rhs_dev, double *u_dev);
+
 /* ---- batched / served instances ------------------------------------- */
 typedef struct lh_batch lh_batch;
 /* A batch owns many independent instances of uneven size that advance in
