@@ -176,6 +176,48 @@ def column_alg_bytes(desc):
     return 20 * F
 
 
+def batched_and_served(args):
+    """Throughput of the batched engine (64 instances of 32x32x153, Re_tau and
+    dt drawn per instance) and of the serving loop on a scaled Poisson stream,
+    next to the plain single-instance path on the same stream."""
+    from lh_b200 import Batch, Desc, grids, perturbed_laminar, re_from_retau
+    from lh_b200.serve import poisson_stream, run_plain, serve
+    rng = np.random.default_rng(20260003)
+    b = Batch()
+    pts = 0
+    for k in range(64):
+        d = Desc(Nx=32, Nz=32, ny=153, Re=re_from_retau(rng.uniform(100, 400), MPGX), mpgx=MPGX, dt_mode=1,
+                 dt=rng.uniform(5e-4, 2e-3))
+        yu, yv = grids(d)
+        b.add(d, *perturbed_laminar(d, 20260003 + 1000 * k, yu, yv))
+        pts += d.points()
+    b.step(3)
+    b.synchronize()
+    K = 10
+    t0 = time.perf_counter()
+    b.step(K)
+    b.synchronize()
+    bt = time.perf_counter() - t0
+    b.close()
+    batched = {"workload": "64 instances of 32x32x153, Re_tau~U[100,400], dt~U[5e-4,2e-3], one launch per "
+                           "kernel class and chunk round per substep, CUDA graph",
+               "value": pts * 3 * K / bt, "unit": UNIT, "ms_per_step": 1e3 * bt / K}
+    n_req = args.serve_requests
+    mk = lambda: poisson_stream(n_req, 4.0, np.random.default_rng(20260005), [32, 64, 128, 192], [97, 153, 257],
+                                steps=(20, 200))
+    reqs = mk()
+    st = serve(reqs, hbm_budget=150 << 30, max_chunk=50, keep_results=False, time_scale=0.25)
+    reqs2 = mk()
+    tp = run_plain(reqs2, keep_results=False)
+    served = {"workload": f"{n_req} requests, Poisson arrivals (4/s, replayed 4x faster), grids "
+                          "{32,64,128,192}^2 x ny {97,153,257}, Re_tau~U[100,550], steps log-U[20,200] "
+                          "(the serving config with 25x shorter requests), 150 GB budget",
+              "value": st.throughput, "unit": UNIT, "p50_ttc_s": st.p50, "p99_ttc_s": st.p99,
+              "mean_live": st.mean_live, "max_live": st.max_live, "wall_s": st.wall,
+              "plain_same_stream": sum(r.work for r in reqs2) / tp}
+    return batched, served
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from lh_b200 import Engine, grids, perturbed_laminar
@@ -245,6 +287,10 @@ def run_ours(args, rank, world, local_rank):
         tdist.all_reduce(te, op=tdist.ReduceOp.MAX)
     e2e_val = world * pts_sub * Ke / float(te.item())
 
+    batched = served = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        batched, served = batched_and_served(args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -265,6 +311,8 @@ def run_ours(args, rank, world, local_rank):
             "kernels_ms_per_step": {k: v[0] / 2 for k, v in prof.items()},
             "dominant_kernel": dom[0],
             "cpu_baseline": cpu,
+            "batched": batched,
+            "served": served,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -278,6 +326,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-serve", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--serve-requests", type=int, default=30)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

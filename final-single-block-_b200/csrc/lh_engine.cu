@@ -321,7 +321,18 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
             it = classes.end() - 1;
         }
         cls_of[q] = (int)(it - classes.begin());
-        rounds = std::max(rounds, (s.nyu + insts[q]->inst.chunk - 1) / insts[q]->inst.chunk);
+    }
+    // Planes per round: the staging of one round, summed over every instance
+    // of the plan, stays inside the L2 budget so staging never reaches HBM.
+    const size_t l2_budget = 40ull << 20;
+    std::vector<int> chunk_eff(insts.size());
+    for (size_t q = 0; q < insts.size(); q++) {
+        const HostSetup &s = insts[q]->hs;
+        const size_t per_plane = (size_t)kNumProducts * s.Mz * s.nxh * sizeof(double2);
+        size_t c = l2_budget / (per_plane * insts.size());
+        c = std::max<size_t>(1, std::min<size_t>(c, (size_t)insts[q]->inst.chunk));
+        chunk_eff[q] = (int)c;
+        rounds = std::max(rounds, (s.nyu + chunk_eff[q] - 1) / chunk_eff[q]);
     }
     const size_t ncls = classes.size();
     std::vector<ClassTiles> tiles(ncls);
@@ -336,7 +347,7 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
     for (int q = 0; q < (int)insts.size(); q++) {
         const HostSetup &s = insts[q]->hs;
         const ClassTiles &ct = tiles[cls_of[q]];
-        const int chunk = insts[q]->inst.chunk;
+        const int chunk = chunk_eff[q];
         const int nbz = (s.nxh + ct.cbz - 1) / ct.cbz;
         const int nbx = (s.Mz + ct.rbx - 1) / ct.rbx;
         const int nbf = (s.nxh + ct.cbf - 1) / ct.cbf;

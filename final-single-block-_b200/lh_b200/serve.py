@@ -1,0 +1,170 @@
+"""Serving loop: simulation requests admitted by HBM budget and advanced
+together with continuous batching.
+
+Requests arrive over time (e.g. a Poisson stream).  The server keeps every
+admitted instance's state resident on the device in one :class:`Batch`;
+between RK3 steps it admits waiting requests while the HBM budget allows,
+advances all live instances in shared launches, and retires instances the
+moment they reach their step count (their memory then admits the next
+requests).  Progress is tracked on the host (each live instance advances by
+exactly the steps the batch takes while it is a member), so no device
+round trip decides completion.  Results are the final states and the
+time-to-completion of every request.
+
+``run_plain`` runs the same requests one at a time through the
+single-instance :class:`Engine` -- the drop-in path -- for comparison.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .capi import Batch, Desc, Engine, LHError, LH_ENOMEM
+from .state import grids, perturbed_laminar, re_from_retau
+
+
+@dataclass
+class Request:
+    rid: int
+    desc: Desc
+    seed: int
+    nsteps: int
+    arrival: float = 0.0  # seconds after the start of the run
+    # filled by the server
+    admitted: float = math.nan
+    finished: float = math.nan
+    result: dict | None = None
+
+    @property
+    def work(self) -> float:
+        """grid-point substeps of the request"""
+        return self.desc.points() * 3.0 * self.nsteps
+
+
+def poisson_stream(n: int, rate: float, rng: np.random.Generator, grid_choices, ny_choices,
+                   retau=(100.0, 550.0), steps=(200, 5000), dt=(5e-4, 2e-3), base_seed: int = 20260005):
+    """Requests with Poisson arrivals, grids and Re_tau drawn as the serving config describes."""
+    t = 0.0
+    out = []
+    for k in range(n):
+        t += rng.exponential(1.0 / rate)
+        N = int(rng.choice(grid_choices))
+        ny = int(rng.choice(ny_choices))
+        rt = float(rng.uniform(*retau))
+        ns = int(round(math.exp(rng.uniform(math.log(steps[0]), math.log(steps[1])))))
+        d = Desc(Nx=N, Nz=N, ny=ny, Re=re_from_retau(rt), dt_mode=1, dt=float(rng.uniform(*dt)))
+        out.append(Request(k, d, base_seed + 1000 * k, max(1, ns), t))
+    return out
+
+
+def initial_state(req: Request):
+    yu, yv = grids(req.desc)
+    return perturbed_laminar(req.desc, req.seed, yu, yv)
+
+
+@dataclass
+class ServeStats:
+    wall: float
+    requests: int
+    work: float
+    p50: float
+    p99: float
+    mean_live: float
+    max_live: int
+    rejected_at_peak: int = 0
+    ttc: list = field(default_factory=list)
+
+    @property
+    def throughput(self) -> float:
+        return self.work / self.wall if self.wall > 0 else 0.0
+
+
+def serve(requests, hbm_budget: int, max_chunk: int = 50, keep_results: bool = True,
+          time_scale: float = 1.0, clock=time.perf_counter, batch_factory=Batch,
+          state_fn=None) -> ServeStats:
+    """Continuous batching over `requests` (sorted by arrival).
+
+    time_scale < 1 compresses the arrival times (a faster replay of the
+    stream); the reported time-to-completion is in real seconds.
+    batch_factory/state_fn default to the device batch and the synthetic
+    initial state; tests substitute host fakes to check the scheduling.
+    """
+    reqs = sorted(requests, key=lambda r: r.arrival)
+    state_fn = state_fn or initial_state
+    b = batch_factory(hbm_budget)
+    queue: list[Request] = []
+    live: dict[int, tuple[Request, int]] = {}  # slot -> (request, remaining steps)
+    nxt = 0
+    t0 = clock()
+    live_samples = []
+    done = 0
+    while done < len(reqs):
+        now = clock() - t0
+        while nxt < len(reqs) and reqs[nxt].arrival * time_scale <= now:
+            queue.append(reqs[nxt])
+            nxt += 1
+        # admit in arrival order while memory allows
+        while queue:
+            r = queue[0]
+            try:
+                slot = b.add(r.desc, *state_fn(r))
+            except LHError as e:
+                if e.code == LH_ENOMEM and live:
+                    break  # wait for a retirement
+                raise
+            r.admitted = clock() - t0
+            live[slot] = (r, r.nsteps)
+            queue.pop(0)
+        if not live:
+            # idle until the next arrival
+            if nxt < len(reqs):
+                wait = reqs[nxt].arrival * time_scale - (clock() - t0)
+                if wait > 0:
+                    time.sleep(min(wait, 0.05))
+            continue
+        k = min(max_chunk, min(rem for _, rem in live.values()))
+        b.step(k)
+        live_samples.append(len(live))
+        finished = []
+        for slot, (r, rem) in list(live.items()):
+            rem -= k
+            if rem == 0:
+                finished.append(slot)
+            live[slot] = (r, rem)
+        if finished:
+            b.synchronize()
+            tf = clock() - t0
+            for slot in finished:
+                r, _ = live.pop(slot)
+                if keep_results:
+                    r.result = b.download(slot)
+                r.finished = tf
+                b.remove(slot)
+                done += 1
+    b.synchronize()
+    wall = clock() - t0
+    ttc = [r.finished - r.arrival * time_scale for r in reqs]
+    b.close()
+    return ServeStats(wall=wall, requests=len(reqs), work=sum(r.work for r in reqs),
+                      p50=float(np.percentile(ttc, 50)), p99=float(np.percentile(ttc, 99)),
+                      mean_live=float(np.mean(live_samples)) if live_samples else 0.0,
+                      max_live=max(live_samples) if live_samples else 0, ttc=ttc)
+
+
+def run_plain(requests, keep_results: bool = True, clock=time.perf_counter) -> float:
+    """The drop-in path: each request alone through the single-instance engine.
+
+    Returns the wall time; states go to ``request.result``."""
+    t0 = clock()
+    for r in requests:
+        e = Engine(r.desc)
+        e.upload(*initial_state(r))
+        e.step(r.nsteps)
+        e.synchronize()
+        if keep_results:
+            r.result = e.download()
+        e.close()
+    return clock() - t0
