@@ -1,23 +1,29 @@
 // Column pass of one RK3 substep: everything that couples a (kx, kz) mode
-// along y.  One thread owns one column and sweeps y four times:
+// along y.  A CTA owns 32 columns (one per lane) and runs three warps on
+// them, one per velocity component (u1, u3, u2), so the three Helmholtz
+// chains of a column advance side by side:
 //
-//   A (up)   RHS0_u1/u2/u3 (littleharsh.f90:682-856, laplacian_U/V :281-368),
-//            the y-flux derivatives and the Nu sum (FOU3D.f90:268-281,
-//            550-590), du += -g Nu (:359-368), the solveU right-hand side
-//            (littleharsh.f90:878-890) and the forward elimination of the
-//            three Helmholtz systems.  The LU factors of LU_build/LU_dec
-//            (tridLU_3D.f90:163-221, 327-364) are formed on the fly; u and w
-//            share one factorisation (the reference rebuilds it per field).
-//   B (down) back substitution (tridLU_3D.f90:80-82), flow-rate correction
-//            for flag_ctpress = 0 (column 0 only, littleharsh.f90:515-548),
-//            divergence and the Poisson right-hand side (:645-658).
-//   C (up)   LUsolP forward sweep with the set-up DG factors (:118-124).
-//   D (down) LUsolP back sweep, p += psi, v_corr and the ghost rows
-//            (littleharsh.f90:896-993).
+//   A (up, all warps)   RHS0_u1/u2/u3 (littleharsh.f90:682-856, laplacian_U/V
+//            :281-368), the y-flux derivatives and the Nu sum (FOU3D.f90:
+//            268-281, 550-590), du += -g Nu (:359-368), the solveU right-hand
+//            side (littleharsh.f90:878-890) and the forward elimination of
+//            that warp's Helmholtz system.  The LU factors of LU_build/LU_dec
+//            (tridLU_3D.f90:163-221, 327-364) are formed on the fly; the u
+//            and w warps form the same u-grid factors with the same
+//            arithmetic, so they agree bit for bit.
+//   B (down, all warps) back substitution (tridLU_3D.f90:80-82).
+//   C (up, u1 warp)     flow-rate correction for flag_ctpress = 0 (column 0
+//            only, littleharsh.f90:515-548), divergence and the Poisson
+//            right-hand side (:645-658), LUsolP forward sweep with the set-up
+//            DG factors (tridLU_3D.f90:118-124).
+//   D1 (down, u1 warp)  LUsolP back sweep and p += psi.
+//   D2 (up, all warps)  v_corr and the ghost rows (littleharsh.f90:896-993).
 //
-// Intermediate y rows are written in place into the state arrays; the
-// scaled upper diagonals go to FACU/FACV for the back substitution.
-#include "lh_core.cuh"
+// Block barriers separate the phases; every lane reaches them, columns past
+// the instance's last only skip the work.  Intermediate y rows are written
+// in place into the state arrays; the scaled upper diagonals go to FACU/FACV
+// for the back substitution.
+#include "lh_kernels.cuh"
 
 namespace lh {
 
@@ -46,9 +52,10 @@ __device__ __forceinline__ double2 cscale(double s, double2 a) { return make_dou
 // cp.async, so a sweep keeps kStages-1 rows of loads in flight while it
 // works on the current row; slots are [stage][slot][lane] so the 32 lanes of
 // a warp touch 512 contiguous bytes.
-constexpr int kColThreads = 32;
+constexpr int kColThreads = kColumnThreads;
+constexpr int kRoles = kColumnBlock / kColumnThreads;
 constexpr int kStages = 8;
-constexpr int kSlotsA = 13, kSlotsB = 4, kSlotsC = 2, kSlotsD = 6;
+constexpr int kSlots = 5;
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void cp16(double2 *s, const double2 *g)
@@ -66,25 +73,46 @@ __device__ __forceinline__ void cp_wait()
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+// Per-thread ring of kStages row stages with kSlots complex slots each,
+// laid out [stage][slot][lane] so a warp's 32 lanes touch 512 contiguous
+// bytes; every warp of the CTA owns one ring.
 struct Ring {
     double2 *base;
-    int nslot, lane;
-    __device__ double2 *at(int stage, int slot) const { return base + ((stage * nslot + slot) * kColThreads + lane); }
+    int lane;
+    __device__ double2 *at(int stage, int slot) const { return base + ((stage * kSlots + slot) * kColThreads + lane); }
 };
 
-size_t column_smem_bytes() { return (size_t)kStages * kSlotsA * kColThreads * sizeof(double2); }
+size_t column_smem_bytes() { return (size_t)kRoles * kStages * kSlots * kColThreads * sizeof(double2); }
 
-__global__ void __launch_bounds__(kColThreads) k_column(const Inst *__restrict__ insts, const Work *__restrict__ work,
-                                                        int kRK)
+// Row streamer: rows are visited in order r = 0..n-1; fill(r, stage) issues
+// the copies of row r.  Keeps kStages-1 rows in flight.
+template <class Fill, class Use>
+__device__ __forceinline__ void stream_rows(int n, Fill &&fill, Use &&use)
+{
+    for (int r = 0; r < kStages - 1; r++) {
+        if (r < n) fill(r, r % kStages);
+        cp_commit();
+    }
+    for (int r = 0; r < n; r++) {
+        cp_wait<kStages - 2>();
+        use(r, r % kStages);
+        if (r + kStages - 1 < n) fill(r + kStages - 1, (r + kStages - 1) % kStages);
+        cp_commit();
+    }
+    cp_wait<0>();
+}
+
+__global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__restrict__ insts,
+                                                                const Work *__restrict__ work, int kRK)
 {
     extern __shared__ double2 ring_mem[];
     const Work w = work[blockIdx.x];
     const Inst &I = insts[w.inst];
-    const int lane = threadIdx.x;
+    const int lane = threadIdx.x % kColThreads, role = threadIdx.x / kColThreads;
     const int col = w.j * kColThreads + lane;
-    if (col >= I.nc) return;  // whole-warp granularity except the last block; no block barriers below
+    const bool live = col < I.nc;  // inactive lanes still reach every barrier
     const int nc = I.nc, nxh = I.nxh, nyu = I.nyu, nyv = I.nyv;
-    const int i = col % nxh, kr = col / nxh;
+    const int i = live ? col % nxh : 0, kr = live ? col / nxh : 0;
     const RK rk = rk_coeffs(kRK);
     const double dt = I.sc[SC_DT];
     const double Re = I.Re;
@@ -92,218 +120,157 @@ __global__ void __launch_bounds__(kColThreads) k_column(const Inst *__restrict__
     const double kxr = I.kx[i], kzr = I.kz[kr];
     const double k2x = I.k2x[i], k2z = I.k2z[kr];
     const double beta = rk.b * dt / Re;
-    // C3 = -dRK*k1F: (-0, -(d k)); C3*p = ((d k) p.im, -((d k) p.re))
-    const double dC3x = rk.d * kxr, dC3z = rk.d * kzr;
     const double ddv = I.ddthetavi;
     const bool mean = (col == 0);
-    const double C1m = -rk.d * I.sc[SC_MPGX];
-
-    double2 *U1 = I.U1 + col, *U2 = I.U2 + col, *U3 = I.U3 + col, *P = I.P + col;
-    double2 *N1 = I.NU1 + col, *N2 = I.NU2 + col, *N3 = I.NU3 + col;
-    const double2 *X1 = I.NXZ1 + col, *X2 = I.NXZ2 + col, *X3 = I.NXZ3 + col;
-    const double2 *UVF = I.UVF + col, *WVF = I.WVF + col, *VVC = I.VVC + col;
-    double *FU = I.FACU + col, *FV = I.FACV + col;
-    double2 *PS = I.PSI + col;
+    const size_t cc = live ? col : 0;
+    double2 *U1 = I.U1 + cc, *U2 = I.U2 + cc, *U3 = I.U3 + cc, *P = I.P + cc;
+    double2 *PS = I.PSI + cc;
+    double *FU = I.FACU + cc, *FV = I.FACV + cc;
     const double *du = I.dyu2i, *dv = I.dyv2i;
+    Ring ring{ring_mem + (size_t)role * kStages * kSlots * kColThreads, lane};
 
     // ---------------- A: right-hand sides and forward elimination --------
-    Ring ra{ring_mem, kSlotsA, lane};
-    auto fillA = [&](int j) {  // inputs of row j (1..nyu)
-        const int st = (j - 1) % kStages;
-        const size_t o = (size_t)j * nc, on = o - nc;
-        cp16(ra.at(st, 0), U1 + o + nc);
-        cp16(ra.at(st, 1), U3 + o + nc);
-        cp16(ra.at(st, 4), N1 + on);
-        cp16(ra.at(st, 5), N3 + on);
-        cp16(ra.at(st, 7), X1 + on);
-        cp16(ra.at(st, 8), X3 + on);
-        cp16(ra.at(st, 10), UVF + o);
-        cp16(ra.at(st, 11), WVF + o);
-        if (j <= nyv) {
-            cp16(ra.at(st, 2), U2 + o + nc);
-            cp16(ra.at(st, 3), P + o);  // p(j+1)
-            cp16(ra.at(st, 6), N2 + on);
-            cp16(ra.at(st, 9), X2 + on);
-            cp16(ra.at(st, 12), VVC + o + nc);
-        }
-    };
-    // row 0: rhs = 0 and a = [0, 1, gw1] (u, w) / [0, 1, 0] (v)
-    double2 u1m = U1[0], u1c = U1[(size_t)nc], u3m = U3[0], u3c = U3[(size_t)nc];
-    double2 u2m = U2[0], u2c = U2[(size_t)nc];
-    double2 uvf_prev = UVF[0], wvf_prev = WVF[0];
-    double2 vvc_c = VVC[(size_t)nc];
-    double2 p_c = P[0];  // p(1)
-    double a3u = I.gw1 * 1.0;
-    double a3v = 0.0 * 1.0;
-    double2 y1p = make_double2(0.0, 0.0), y3p = y1p, y2p = y1p;
-    for (int r = 0; r < kStages - 1; r++) {
-        if (1 + r <= nyu) fillA(1 + r);
-        cp_commit();
-    }
-    U1[0] = y1p;
-    U3[0] = y3p;
-    U2[0] = y2p;
-    FU[0] = a3u;
-    FV[0] = a3v;
-    for (int j = 1; j <= nyu; j++) {
-        cp_wait<kStages - 2>();
-        const int st = (j - 1) % kStages;
-        const size_t o = (size_t)j * nc;
-        const size_t on = o - nc;
-        const double2 u1p = *ra.at(st, 0), u3p = *ra.at(st, 1);
-        const double2 n1o = *ra.at(st, 4), n3o = *ra.at(st, 5);
-        const double2 x1 = *ra.at(st, 7), x3 = *ra.at(st, 8);
-        const double2 uvf = *ra.at(st, 10), wvf = *ra.at(st, 11);
-        double2 u2p, p_n, n2o, x2, vvn;
-        if (j <= nyv) {
-            u2p = *ra.at(st, 2);
-            p_n = *ra.at(st, 3);
-            n2o = *ra.at(st, 6);
-            x2 = *ra.at(st, 9);
-            vvn = *ra.at(st, 12);
-        }
-        if (j + kStages - 1 <= nyu) fillA(j + kStages - 1);
-        cp_commit();
-
-        const double d1 = du[3 * j], d2 = du[3 * j + 1], d3 = du[3 * j + 2];
-        const double cen = k2x + k2z + d2;
-        double2 L1 = make_double2(d1 * u1m.x + cen * u1c.x + d3 * u1p.x, d1 * u1m.y + cen * u1c.y + d3 * u1p.y);
-        double2 L3 = make_double2(d1 * u3m.x + cen * u3c.x + d3 * u3p.x, d1 * u3m.y + cen * u3c.y + d3 * u3p.y);
-        double2 du1 = make_double2(C1 * L1.x + C2 * n1o.x + dC3x * p_c.y, C1 * L1.y + C2 * n1o.y + -(dC3x * p_c.x));
-        double2 du3 = make_double2(C1 * L3.x + C2 * n3o.x + dC3z * p_c.y, C1 * L3.y + C2 * n3o.y + -(dC3z * p_c.x));
-        if (mean) du1.x = du1.x + C1m;
-        const double m = I.dthdyu[j];
-        const double2 nu1 = make_double2(x1.x + (uvf.x - uvf_prev.x) * m * ddv, x1.y + (uvf.y - uvf_prev.y) * m * ddv);
-        const double2 nu3 = make_double2(x3.x + (wvf.x - wvf_prev.x) * m * ddv, x3.y + (wvf.y - wvf_prev.y) * m * ddv);
-        N1[on] = nu1;
-        N3[on] = nu3;
-        du1 = make_double2(du1.x + G * nu1.x, du1.y + G * nu1.y);
-        du3 = make_double2(du3.x + G * nu3.x, du3.y + G * nu3.y);
-        const double2 r1 = make_double2(u1c.x + dt * du1.x, u1c.y + dt * du1.y);
-        const double2 r3 = make_double2(u3c.x + dt * du3.x, u3c.y + dt * du3.y);
-        const double a1 = -beta * d1;
-        const double a2 = 1.0 - beta * (d2 + k2x + k2z);
-        const double a3 = -beta * d3;
-        const double inv = 1.0 / (a2 - a1 * a3u);
-        const double2 y1 = make_double2((r1.x - a1 * y1p.x) * inv, (r1.y - a1 * y1p.y) * inv);
-        const double2 y3 = make_double2((r3.x - a1 * y3p.x) * inv, (r3.y - a1 * y3p.y) * inv);
-        a3u = a3 * inv;
-        U1[o] = y1;
-        U3[o] = y3;
-        FU[o] = a3u;
-        y1p = y1;
-        y3p = y3;
-        u1m = u1c;
-        u1c = u1p;
-        u3m = u3c;
-        u3c = u3p;
-        uvf_prev = uvf;
-        wvf_prev = wvf;
-        if (j <= nyv) {
-            const double e1 = dv[3 * j], e2 = dv[3 * j + 1], e3 = dv[3 * j + 2];
-            const double cenv = k2x + k2z + e2;
-            const double2 L2 = make_double2(e1 * u2m.x + cenv * u2c.x + e3 * u2p.x, e1 * u2m.y + cenv * u2c.y + e3 * u2p.y);
-            const double mv = I.dthdyv[j];
-            const double C3 = -rk.d * ddv * mv;
-            double2 du2 = make_double2(C1 * L2.x + C2 * n2o.x + C3 * (p_n.x - p_c.x),
-                                       C1 * L2.y + C2 * n2o.y + C3 * (p_n.y - p_c.y));
-            const double2 nu2 = make_double2(x2.x + (vvn.x - vvc_c.x) * mv * ddv, x2.y + (vvn.y - vvc_c.y) * mv * ddv);
-            N2[on] = nu2;
-            du2 = make_double2(du2.x + G * nu2.x, du2.y + G * nu2.y);
-            const double2 r2 = make_double2(u2c.x + dt * du2.x, u2c.y + dt * du2.y);
-            const double b1 = -beta * e1;
-            const double b2 = 1.0 - beta * (e2 + k2x + k2z);
-            const double b3 = -beta * e3;
-            const double invv = 1.0 / (b2 - b1 * a3v);
-            const double2 y2 = make_double2((r2.x - b1 * y2p.x) * invv, (r2.y - b1 * y2p.y) * invv);
-            a3v = b3 * invv;
-            U2[o] = y2;
-            FV[o] = a3v;
-            y2p = y2;
-            u2m = u2c;
-            u2c = u2p;
-            vvc_c = vvn;
-            p_c = p_n;
-        }
-    }
-    cp_wait<0>();
-    // top rows, rhs = 0: u/w a = [gw2, 1, 0], v a = [0, 1, 0]
-    {
+    if (live && role < 2) {
+        // u1 (role 0) or u3 (role 1): RHS0_u1/u3 (littleharsh.f90:682-751,
+        // 807-856), Nu sum (FOU3D.f90:268-281), du += -g Nu (:359-364),
+        // solveU rhs (littleharsh.f90:878-890), LU_build/LU_dec on the fly;
+        // both roles form the same u-grid factors with the same arithmetic.
+        double2 *U = role == 0 ? U1 : U3;
+        double2 *N = (role == 0 ? I.NU1 : I.NU3) + cc;
+        const double2 *X = (role == 0 ? I.NXZ1 : I.NXZ3) + cc;
+        const double2 *FL = (role == 0 ? I.UVF : I.WVF) + cc;
+        // C3 = -dRK*k1F: (-0, -(d k)); C3*p = ((d k) p.im, -((d k) p.re))
+        const double dC3 = rk.d * (role == 0 ? kxr : kzr);
+        const double C1m = (role == 0 && mean) ? -rk.d * I.sc[SC_MPGX] : 0.0;
+        double2 um = U[0], uc = U[(size_t)nc];
+        double2 flp = FL[0];
+        double a3u = I.gw1 * 1.0;
+        double2 yp = make_double2(0.0, 0.0);
+        U[0] = yp;
+        if (role == 0) FU[0] = a3u;
+        stream_rows(nyu,
+                    [&](int r, int st) {
+                        const int j = r + 1;
+                        const size_t o = (size_t)j * nc, on = o - nc;
+                        cp16(ring.at(st, 0), U + o + nc);
+                        cp16(ring.at(st, 1), P + on);
+                        cp16(ring.at(st, 2), N + on);
+                        cp16(ring.at(st, 3), X + on);
+                        cp16(ring.at(st, 4), FL + o);
+                    },
+                    [&](int r, int st) {
+                        const int j = r + 1;
+                        const size_t o = (size_t)j * nc, on = o - nc;
+                        const double2 up = *ring.at(st, 0), pj = *ring.at(st, 1), no = *ring.at(st, 2);
+                        const double2 x = *ring.at(st, 3), fl = *ring.at(st, 4);
+                        const double d1 = du[3 * j], d2 = du[3 * j + 1], d3 = du[3 * j + 2];
+                        const double cen = k2x + k2z + d2;
+                        const double2 L = make_double2(d1 * um.x + cen * uc.x + d3 * up.x, d1 * um.y + cen * uc.y + d3 * up.y);
+                        double2 dd = make_double2(C1 * L.x + C2 * no.x + dC3 * pj.y, C1 * L.y + C2 * no.y + -(dC3 * pj.x));
+                        if (role == 0 && mean) dd.x = dd.x + C1m;
+                        const double m = I.dthdyu[j];
+                        const double2 nu = make_double2(x.x + (fl.x - flp.x) * m * ddv, x.y + (fl.y - flp.y) * m * ddv);
+                        N[on] = nu;
+                        dd = make_double2(dd.x + G * nu.x, dd.y + G * nu.y);
+                        const double2 rh = make_double2(uc.x + dt * dd.x, uc.y + dt * dd.y);
+                        const double a1 = -beta * d1;
+                        const double a2 = 1.0 - beta * (d2 + k2x + k2z);
+                        const double a3 = -beta * d3;
+                        const double inv = 1.0 / (a2 - a1 * a3u);
+                        const double2 y = make_double2((rh.x - a1 * yp.x) * inv, (rh.y - a1 * yp.y) * inv);
+                        a3u = a3 * inv;
+                        U[o] = y;
+                        if (role == 0) FU[o] = a3u;
+                        yp = y;
+                        um = uc;
+                        uc = up;
+                        flp = fl;
+                    });
+        // top row: a = [gw2, 1, 0], rhs = 0
         const double inv = 1.0 / (1.0 - I.gw2 * a3u);
-        const double2 y1 = make_double2((0.0 - I.gw2 * y1p.x) * inv, (0.0 - I.gw2 * y1p.y) * inv);
-        const double2 y3 = make_double2((0.0 - I.gw2 * y3p.x) * inv, (0.0 - I.gw2 * y3p.y) * inv);
-        U1[(size_t)(nyu + 1) * nc] = y1;
-        U3[(size_t)(nyu + 1) * nc] = y3;
-        y1p = y1;
-        y3p = y3;
-        const double invv = 1.0 / (1.0 - 0.0 * a3v);
-        const double2 y2 = make_double2((0.0 - 0.0 * y2p.x) * invv, (0.0 - 0.0 * y2p.y) * invv);
-        U2[(size_t)(nyv + 1) * nc] = y2;
-        y2p = y2;
+        U[(size_t)(nyu + 1) * nc] = make_double2((0.0 - I.gw2 * yp.x) * inv, (0.0 - I.gw2 * yp.y) * inv);
+    } else if (live && role == 2) {
+        // u2: RHS0_u2 (littleharsh.f90:753-805) with laplacian_V, Nu2 sum,
+        // solveU on the v grid
+        double2 *N = I.NU2 + cc;
+        const double2 *X = I.NXZ2 + cc;
+        const double2 *VV = I.VVC + cc;
+        double2 um = U2[0], uc = U2[(size_t)nc];
+        double2 vvc = VV[(size_t)nc];
+        double2 pc = P[0];
+        double a3v = 0.0 * 1.0;
+        double2 yp = make_double2(0.0, 0.0);
+        U2[0] = yp;
+        FV[0] = a3v;
+        stream_rows(nyv,
+                    [&](int r, int st) {
+                        const int j = r + 1;
+                        const size_t o = (size_t)j * nc, on = o - nc;
+                        cp16(ring.at(st, 0), U2 + o + nc);
+                        cp16(ring.at(st, 1), P + o);  // p(j+1)
+                        cp16(ring.at(st, 2), N + on);
+                        cp16(ring.at(st, 3), X + on);
+                        cp16(ring.at(st, 4), VV + o + nc);
+                    },
+                    [&](int r, int st) {
+                        const int j = r + 1;
+                        const size_t o = (size_t)j * nc, on = o - nc;
+                        const double2 up = *ring.at(st, 0), pn = *ring.at(st, 1), no = *ring.at(st, 2);
+                        const double2 x = *ring.at(st, 3), vvn = *ring.at(st, 4);
+                        const double e1 = dv[3 * j], e2 = dv[3 * j + 1], e3 = dv[3 * j + 2];
+                        const double cenv = k2x + k2z + e2;
+                        const double2 L = make_double2(e1 * um.x + cenv * uc.x + e3 * up.x, e1 * um.y + cenv * uc.y + e3 * up.y);
+                        const double mv = I.dthdyv[j];
+                        const double C3 = -rk.d * ddv * mv;
+                        double2 dd = make_double2(C1 * L.x + C2 * no.x + C3 * (pn.x - pc.x), C1 * L.y + C2 * no.y + C3 * (pn.y - pc.y));
+                        const double2 nu = make_double2(x.x + (vvn.x - vvc.x) * mv * ddv, x.y + (vvn.y - vvc.y) * mv * ddv);
+                        N[on] = nu;
+                        dd = make_double2(dd.x + G * nu.x, dd.y + G * nu.y);
+                        const double2 rh = make_double2(uc.x + dt * dd.x, uc.y + dt * dd.y);
+                        const double b1 = -beta * e1;
+                        const double b2 = 1.0 - beta * (e2 + k2x + k2z);
+                        const double b3 = -beta * e3;
+                        const double inv = 1.0 / (b2 - b1 * a3v);
+                        const double2 y = make_double2((rh.x - b1 * yp.x) * inv, (rh.y - b1 * yp.y) * inv);
+                        a3v = b3 * inv;
+                        U2[o] = y;
+                        FV[o] = a3v;
+                        yp = y;
+                        um = uc;
+                        uc = up;
+                        vvc = vvn;
+                        pc = pn;
+                    });
+        const double inv = 1.0 / (1.0 - 0.0 * a3v);
+        U2[(size_t)(nyv + 1) * nc] = make_double2((0.0 - 0.0 * yp.x) * inv, (0.0 - 0.0 * yp.y) * inv);
     }
-    __threadfence_block();
+    __syncthreads();
 
-    // ---------------- B: back substitution and divergence ---------------
+    // ---------------- B: back substitution (tridLU_3D.f90:80-82) ----------
+    if (live) {
+        double2 *U = role == 0 ? U1 : (role == 1 ? U3 : U2);
+        const double *F = role == 2 ? FV : FU;
+        const int top = role == 2 ? nyv + 1 : nyu + 1;
+        double2 v = U[(size_t)top * nc];
+        stream_rows(top,
+                    [&](int r, int st) {
+                        const int j = top - 1 - r;
+                        cp16(ring.at(st, 0), U + (size_t)j * nc);
+                        cp8(&ring.at(st, 1)->x, F + (size_t)j * nc);
+                    },
+                    [&](int r, int st) {
+                        const int j = top - 1 - r;
+                        const double2 y = *ring.at(st, 0);
+                        const double f = ring.at(st, 1)->x;
+                        v = make_double2(y.x - f * v.x, y.y - f * v.y);
+                        U[(size_t)j * nc] = v;
+                    });
+    }
+    __syncthreads();
+
     const double dtirk = (1.0 / dt) / (rk.a + rk.b);
-    const bool div_inline = I.flag_ctpress != 0;
-    Ring rb{ring_mem, kSlotsB, lane};
-    auto fillB = [&](int j) {  // row j (nyu .. 0)
-        const int st = (nyu - j) % kStages;
-        const size_t o = (size_t)j * nc;
-        cp16(rb.at(st, 0), U1 + o);
-        cp16(rb.at(st, 1), U3 + o);
-        cp8(&rb.at(st, 3)->x, FU + o);
-        if (j <= nyv) {
-            cp16(rb.at(st, 2), U2 + o);
-            cp8(&rb.at(st, 3)->y, FV + o);
-        }
-    };
-    for (int r = 0; r < kStages - 1; r++) {
-        if (nyu - r >= 0) fillB(nyu - r);
-        cp_commit();
-    }
-    double2 v1 = y1p, v3 = y3p;  // rows j+1 of u1, u3
-    double2 v2 = y2p;            // u2 at row nyv+1 = nyu
-    for (int j = nyu; j >= 0; j--) {
-        cp_wait<kStages - 2>();
-        const int st = (nyu - j) % kStages;
-        const size_t o = (size_t)j * nc;
-        const double2 y1 = *rb.at(st, 0), y3 = *rb.at(st, 1);
-        const double2 ff = *rb.at(st, 3);
-        double2 y2 = make_double2(0.0, 0.0);
-        if (j <= nyv) y2 = *rb.at(st, 2);
-        if (j - (kStages - 1) >= 0) fillB(j - (kStages - 1));
-        cp_commit();
-        const double f = ff.x;
-        const double2 n1 = make_double2(y1.x - f * v1.x, y1.y - f * v1.y);
-        const double2 n3 = make_double2(y3.x - f * v3.x, y3.y - f * v3.y);
-        U1[o] = n1;
-        U3[o] = n3;
-        double2 n2 = v2;
-        if (j <= nyv) {
-            const double fv = ff.y;
-            n2 = make_double2(y2.x - fv * v2.x, y2.y - fv * v2.y);
-            U2[o] = n2;
-        }
-        if (div_inline && j + 1 <= nyu) {
-            // div(j+1) = i kx u1 + i kz u3 + dthdyu (u2(j+1) - u2(j)), psi = dtirk div
-            const int jp = j + 1;
-            const double mm = ddv * I.dthdyu[jp];
-            const double2 d = make_double2(-(kxr * v1.y) + -(kzr * v3.y) + mm * (v2.x - n2.x),
-                                           kxr * v1.x + kzr * v3.x + mm * (v2.y - n2.y));
-            double2 ps = cscale(dtirk, d);
-            if (mean && jp == 1) ps = make_double2(0.0, 0.0);  // gauge, littleharsh.f90:656-658
-            PS[(size_t)(jp - 1) * nc] = ps;
-        }
-        v1 = n1;
-        v3 = n3;
-        v2 = n2;
-    }
-    cp_wait<0>();
-
-    if (!div_inline) {
-        __threadfence_block();
-        if (mean) {
+    if (live && role == 0) {
+        if (I.flag_ctpress == 0 && mean) {
             // flowrate_corr (littleharsh.f90:515-548): u11 from LUsol0 with
             // LU_build0 (tridLU_3D.f90:299-325); flowrateRe's dummy
             // u(1:nn+2) receives u11(0:nn+2), so it sums u11(j-1).
@@ -349,119 +316,125 @@ __global__ void __launch_bounds__(kColThreads) k_column(const Inst *__restrict__
                 u.x = u.x + g * u11[j];
                 U1[(size_t)j * nc] = u;
             }
+            __threadfence_block();
         }
+        // ---------------- C: divergence and the LUsolP forward sweep -------
+        // psi = div/(dt (a+b)) (littleharsh.f90:645-658), gauge psi(1) = 0 on
+        // mode (0,0), forward elimination with the DG factors (tridLU_3D.f90:118-124)
+        const double *G2 = I.DG2 + cc;
         double2 v2m = U2[0];
-        for (int jp = 1; jp <= nyu; jp++) {
-            const double2 a = U1[(size_t)jp * nc], c3 = U3[(size_t)jp * nc];
-            const double2 v2c = U2[(size_t)jp * nc];
-            const double mm = ddv * I.dthdyu[jp];
-            const double2 d = make_double2(-(kxr * a.y) + -(kzr * c3.y) + mm * (v2c.x - v2m.x),
-                                           kxr * a.x + kzr * c3.x + mm * (v2c.y - v2m.y));
-            double2 ps = cscale(dtirk, d);
-            if (mean && jp == 1) ps = make_double2(0.0, 0.0);
-            PS[(size_t)(jp - 1) * nc] = ps;
-            v2m = v2c;
-        }
-    }
-    __threadfence_block();
-
-    // ---------------- C: LUsolP forward sweep ------------------------------
-    const double *G2 = I.DG2 + col, *G3 = I.DG3 + col;
-    Ring rc{ring_mem, kSlotsC, lane};
-    auto fillC = [&](int j) {  // row j (2 .. nyu)
-        const int st = (j - 2) % kStages;
-        const size_t o = (size_t)(j - 1) * nc;
-        cp16(rc.at(st, 0), PS + o);
-        cp8(&rc.at(st, 1)->x, G2 + o);
-    };
-    for (int r = 0; r < kStages - 1; r++) {
-        if (2 + r <= nyu) fillC(2 + r);
-        cp_commit();
-    }
-    double2 xp = cscale(G2[0], PS[0]);
-    PS[0] = xp;
-    for (int j = 2; j <= nyu; j++) {
-        cp_wait<kStages - 2>();
-        const int st = (j - 2) % kStages;
-        const double2 x = *rc.at(st, 0);
-        const double g2 = rc.at(st, 1)->x;
-        if (j + kStages - 1 <= nyu) fillC(j + kStages - 1);
-        cp_commit();
-        const double g1 = I.DG1[j];
-        xp = make_double2((x.x - g1 * xp.x) * g2, (x.y - g1 * xp.y) * g2);
-        PS[(size_t)(j - 1) * nc] = xp;
-    }
-    cp_wait<0>();
-    __threadfence_block();
-
-    // ---------------- D: LUsolP back sweep, p += psi, v_corr --------------
-    const double dtrk = dt * (rk.a + rk.b);
-    const double kxd = dtrk * kxr, kzd = dtrk * kzr;
-    const double dtrk_u2 = dtrk * ddv;
-    Ring rd{ring_mem, kSlotsD, lane};
-    auto fillD = [&](int j) {  // row j (nyu .. 1)
-        const int st = (nyu - j) % kStages;
-        const size_t o = (size_t)(j - 1) * nc, ou = (size_t)j * nc;
-        cp16(rd.at(st, 0), PS + o);
-        cp16(rd.at(st, 1), P + o);
-        cp16(rd.at(st, 2), U1 + ou);
-        cp16(rd.at(st, 3), U3 + ou);
-        if (j <= nyv) cp16(rd.at(st, 4), U2 + ou);
-        if (j < nyu) cp8(&rd.at(st, 5)->x, G3 + o);
-    };
-    for (int r = 0; r < kStages - 1; r++) {
-        if (nyu - r >= 1) fillD(nyu - r);
-        cp_commit();
-    }
-    double2 psn = make_double2(0.0, 0.0);  // psi(j+1)
-    bool bad = false;
-    for (int j = nyu; j >= 1; j--) {
-        cp_wait<kStages - 2>();
-        const int st = (nyu - j) % kStages;
-        const double2 x = *rd.at(st, 0), p = *rd.at(st, 1);
-        double2 a = *rd.at(st, 2), c3 = *rd.at(st, 3);
-        double2 v = make_double2(0.0, 0.0);
-        if (j <= nyv) v = *rd.at(st, 4);
-        const double g3 = rd.at(st, 5)->x;
-        if (j - (kStages - 1) >= 1) fillD(j - (kStages - 1));
-        cp_commit();
-        const size_t o = (size_t)(j - 1) * nc;
-        double2 ps = x;  // psi(nyu) = x(nyu)
-        if (j < nyu) ps = make_double2(x.x - g3 * psn.x, x.y - g3 * psn.y);
-        PS[o] = ps;
-        P[o] = make_double2(p.x + ps.x, p.y + ps.y);
-        const size_t ou = (size_t)j * nc;
-        a = make_double2(a.x - -(kxd * ps.y), a.y - kxd * ps.x);
-        c3 = make_double2(c3.x - -(kzd * ps.y), c3.y - kzd * ps.x);
-        U1[ou] = a;
-        U3[ou] = c3;
-        if (j == nyu) {
-            U1[ou + nc] = cscale(I.gwbc, a);
-            U3[ou + nc] = cscale(I.gwbc, c3);
-        }
-        if (j == 1) {
-            U1[0] = cscale(I.gwbc, a);
-            U3[0] = cscale(I.gwbc, c3);
-            bad = !isfinite(a.x) || !isfinite(a.y) || !isfinite(ps.x) || !isfinite(ps.y);
-        }
-        if (j <= nyv) {
-            const double mv = dtrk_u2 * I.dthdyv[j];
-            v = make_double2(v.x - mv * (psn.x - ps.x), v.y - mv * (psn.y - ps.y));
-            U2[ou] = v;
-        }
-        psn = ps;
-    }
-    cp_wait<0>();
-    U2[0] = make_double2(0.0, 0.0);
-    U2[(size_t)(nyv + 1) * nc] = make_double2(0.0, 0.0);
-    if (bad) atomicOr(I.err, ERR_NONFINITE);
-    if (mean && kRK == 3) {
-        // flowrateIm (littleharsh.f90:473-492) via meanflow_ctP (:572-589)
+        double2 xp = make_double2(0.0, 0.0);
+        stream_rows(nyu,
+                    [&](int r, int st) {
+                        const int j = r + 1;
+                        const size_t o = (size_t)j * nc;
+                        cp16(ring.at(st, 0), U1 + o);
+                        cp16(ring.at(st, 1), U3 + o);
+                        cp16(ring.at(st, 2), U2 + o);
+                        cp8(&ring.at(st, 3)->x, G2 + o - nc);
+                    },
+                    [&](int r, int st) {
+                        const int j = r + 1;
+                        const double2 a = *ring.at(st, 0), c3 = *ring.at(st, 1), v2c = *ring.at(st, 2);
+                        const double g2 = ring.at(st, 3)->x;
+                        const double mm = ddv * I.dthdyu[j];
+                        const double2 d = make_double2(-(kxr * a.y) + -(kzr * c3.y) + mm * (v2c.x - v2m.x),
+                                                       kxr * a.x + kzr * c3.x + mm * (v2c.y - v2m.y));
+                        double2 ps = cscale(dtirk, d);
+                        if (mean && j == 1) ps = make_double2(0.0, 0.0);
+                        if (j == 1) {
+                            xp = cscale(g2, ps);
+                        } else {
+                            const double g1 = I.DG1[j];
+                            xp = make_double2((ps.x - g1 * xp.x) * g2, (ps.y - g1 * xp.y) * g2);
+                        }
+                        PS[(size_t)(j - 1) * nc] = xp;
+                        v2m = v2c;
+                    });
         __threadfence_block();
-        double Qu = 0.0;
-        for (int j = 1; j <= nyv + 1; j++) Qu = Qu + (I.yv[j] - I.yv[j - 1]) * U1[(size_t)j * nc].x;
-        I.sc[SC_QX] = Qu;
-        I.sc[SC_ITER] = I.sc[SC_ITER] + 1.0;
+        // ---------------- D1: LUsolP back sweep and p += psi ---------------
+        const double *G3 = I.DG3 + cc;
+        double2 psn = xp;  // psi(nyu) = x(nyu)
+        stream_rows(nyu,
+                    [&](int r, int st) {
+                        const int j = nyu - r;
+                        const size_t o = (size_t)(j - 1) * nc;
+                        cp16(ring.at(st, 0), PS + o);
+                        cp16(ring.at(st, 1), P + o);
+                        if (j < nyu) cp8(&ring.at(st, 2)->x, G3 + o);
+                    },
+                    [&](int r, int st) {
+                        const int j = nyu - r;
+                        const size_t o = (size_t)(j - 1) * nc;
+                        const double2 x = *ring.at(st, 0), p = *ring.at(st, 1);
+                        double2 ps = x;
+                        if (j < nyu) {
+                            const double g3 = ring.at(st, 2)->x;
+                            ps = make_double2(x.x - g3 * psn.x, x.y - g3 * psn.y);
+                        }
+                        PS[o] = ps;
+                        P[o] = make_double2(p.x + ps.x, p.y + ps.y);
+                        psn = ps;
+                    });
+    }
+    __syncthreads();
+
+    // ---------------- D2: v_corr (littleharsh.f90:896-993) ------------------
+    const double dtrk = dt * (rk.a + rk.b);
+    if (live && role < 2) {
+        double2 *U = role == 0 ? U1 : U3;
+        const double kd = dtrk * (role == 0 ? kxr : kzr);
+        double2 first = make_double2(0.0, 0.0), last = first, ps1 = first;
+        stream_rows(nyu,
+                    [&](int r, int st) {
+                        const int j = r + 1;
+                        cp16(ring.at(st, 0), U + (size_t)j * nc);
+                        cp16(ring.at(st, 1), PS + (size_t)(j - 1) * nc);
+                    },
+                    [&](int r, int st) {
+                        const int j = r + 1;
+                        double2 a = *ring.at(st, 0);
+                        const double2 ps = *ring.at(st, 1);
+                        a = make_double2(a.x - -(kd * ps.y), a.y - kd * ps.x);
+                        U[(size_t)j * nc] = a;
+                        if (j == 1) {
+                            first = a;
+                            ps1 = ps;
+                        }
+                        if (j == nyu) last = a;
+                    });
+        U[0] = cscale(I.gwbc, first);
+        U[(size_t)(nyu + 1) * nc] = cscale(I.gwbc, last);
+        if (!isfinite(first.x) || !isfinite(first.y) || !isfinite(ps1.x) || !isfinite(ps1.y))
+            atomicOr(I.err, ERR_NONFINITE);
+        if (role == 0 && mean && kRK == 3) {
+            // flowrateIm (littleharsh.f90:473-492) via meanflow_ctP (:572-589)
+            __threadfence_block();
+            double Qu = 0.0;
+            for (int j = 1; j <= nyv + 1; j++) Qu = Qu + (I.yv[j] - I.yv[j - 1]) * U1[(size_t)j * nc].x;
+            I.sc[SC_QX] = Qu;
+            I.sc[SC_ITER] = I.sc[SC_ITER] + 1.0;
+        }
+    } else if (live && role == 2) {
+        const double dtrk_u2 = dtrk * ddv;
+        double2 psc = PS[0];  // psi(j) of the current row
+        stream_rows(nyv,
+                    [&](int r, int st) {
+                        const int j = r + 1;
+                        cp16(ring.at(st, 0), U2 + (size_t)j * nc);
+                        cp16(ring.at(st, 1), PS + (size_t)j * nc);  // psi(j+1)
+                    },
+                    [&](int r, int st) {
+                        const int j = r + 1;
+                        double2 v = *ring.at(st, 0);
+                        const double2 psn = *ring.at(st, 1);
+                        const double mv = dtrk_u2 * I.dthdyv[j];
+                        v = make_double2(v.x - mv * (psn.x - psc.x), v.y - mv * (psn.y - psc.y));
+                        U2[(size_t)j * nc] = v;
+                        psc = psn;
+                    });
+        U2[0] = make_double2(0.0, 0.0);
+        U2[(size_t)(nyv + 1) * nc] = make_double2(0.0, 0.0);
     }
 }
 

@@ -464,7 +464,7 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
         if ((e = time_end(timer, 3, st)) != cudaSuccess) return e;
     }
     time_begin(timer, st);
-    k_column<<<(unsigned)p.column.size(), kColumnThreads, p.sm_col, st>>>(d_insts, p.d_work + p.off_column, kRK);
+    k_column<<<(unsigned)p.column.size(), kColumnBlock, p.sm_col, st>>>(d_insts, p.d_work + p.off_column, kRK);
     if ((e = time_end(timer, 4, st)) != cudaSuccess) return e;
     return cudaGetLastError();
 }

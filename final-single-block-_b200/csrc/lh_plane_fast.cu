@@ -6,6 +6,11 @@
 // template each, instantiated for the Ngal sizes of the usual grids.
 // Twiddles are copied once per CTA into shared memory.
 #include "lh_fft.cuh"
+
+// resident CTAs per SM the register allocation is sized for
+#ifndef LH_FFT_MINB
+#define LH_FFT_MINB 2
+#endif
 #include "lh_kernels.cuh"
 
 namespace lh {
@@ -13,7 +18,7 @@ namespace lh {
 // ---------------------------------------------------------------------------
 // z inverse of one (plane, field, block of cb x modes)
 template <int NZ>
-__global__ void __launch_bounds__(512) k_zinv_f(const Inst *__restrict__ insts, const Work *__restrict__ work, int cb)
+__global__ void __launch_bounds__(512, LH_FFT_MINB) k_zinv_f(const Inst *__restrict__ insts, const Work *__restrict__ work, int cb)
 {
     constexpr int N1 = Plan2<NZ>::N1, N2 = Plan2<NZ>::N2;
     constexpr int Nz = 2 * NZ / 3;
@@ -93,7 +98,7 @@ __global__ void __launch_bounds__(512) k_zinv_f(const Inst *__restrict__ insts, 
 // ---------------------------------------------------------------------------
 // x transforms and products of one (plane, block of rb z rows)
 template <int NX>
-__global__ void __launch_bounds__(512) k_xprod_f(const Inst *__restrict__ insts, const Work *__restrict__ work, int rb,
+__global__ void __launch_bounds__(512, LH_FFT_MINB) k_xprod_f(const Inst *__restrict__ insts, const Work *__restrict__ work, int rb,
                                                  int want_max)
 {
     constexpr int N1 = Plan2<NX>::N1, N2 = Plan2<NX>::N2;
@@ -110,17 +115,24 @@ __global__ void __launch_bounds__(512) k_xprod_f(const Inst *__restrict__ insts,
     __syncthreads();
     const int t = threadIdx.x, v = t % nv, r = t / nv;
     const int pr = v / rb, rr = v % rb, q = q0 + rr;
-    const bool rowok = q < Mz;
+    (void)q;
+    // (0) coalesced load of the 6 fields x rb rows x (Nx/2+1) modes: in[f][rr][k]
+    double2 *in = buf;
+    for (int e = t; e < kNumProducts * rb * nxh; e += blockDim.x) {
+        const int k = e % nxh, fr = e / nxh, rr2 = fr % rb, f = fr / rb;
+        in[e] = (q0 + rr2 < Mz) ? S[((size_t)f * Mz + q0 + rr2) * nxh + k] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
     // (1) inverse pass 1 on the Hermitian extension of two half spectra
-    if (r < N2) {
-        const int fa = pr == 0 ? 0 : (pr == 1 ? 1 : 3), fb = pr == 0 ? 2 : (pr == 1 ? 4 : 5);
-        const double2 *A = S + ((size_t)fa * Mz + q) * nxh, *B = S + ((size_t)fb * Mz + q) * nxh;
+    {
         double2 a[N1];
+        if (r < N2) {
+            const int fa = pr == 0 ? 0 : (pr == 1 ? 1 : 3), fb = pr == 0 ? 2 : (pr == 1 ? 4 : 5);
+            const double2 *A = in + (fa * rb + rr) * nxh, *B = in + (fb * rb + rr) * nxh;
 #pragma unroll
-        for (int n1 = 0; n1 < N1; n1++) {
-            const int n = r + N2 * n1;
-            double2 z = make_double2(0.0, 0.0);
-            if (rowok) {
+            for (int n1 = 0; n1 < N1; n1++) {
+                const int n = r + N2 * n1;
+                double2 z = make_double2(0.0, 0.0);
                 if (n == 0) {
                     z = make_double2(A[0].x, B[0].x);  // Im of mode 0 dropped (rft_buff.f:78-81)
                 } else if (n < nxh) {
@@ -130,15 +142,18 @@ __global__ void __launch_bounds__(512) k_xprod_f(const Inst *__restrict__ insts,
                     const double2 x = A[NX - n], y = B[NX - n];
                     z = make_double2(x.x + y.y, y.x - x.y);
                 }
+                a[n1] = z;
             }
-            a[n1] = z;
         }
-        DFT<N1, +1, NX>::run(a, tw);
+        __syncthreads();
+        if (r < N2) {
+            DFT<N1, +1, NX>::run(a, tw);
 #pragma unroll
-        for (int k1 = 0; k1 < N1; k1++) {
-            double2 z = a[k1];
-            if (k1 > 0 && r > 0) z = twiddle<+1>(tw[r * k1], z);
-            buf[(k1 * N2 + r) * nv + v] = z;
+            for (int k1 = 0; k1 < N1; k1++) {
+                double2 z = a[k1];
+                if (k1 > 0 && r > 0) z = twiddle<+1>(tw[r * k1], z);
+                buf[(k1 * N2 + r) * nv + v] = z;
+            }
         }
     }
     __syncthreads();
@@ -250,7 +265,7 @@ __global__ void __launch_bounds__(512) k_xprod_f(const Inst *__restrict__ insts,
 // ---------------------------------------------------------------------------
 // z forward, masks and derivatives of one (plane, block of cb x modes)
 template <int NZ>
-__global__ void __launch_bounds__(512) k_zfwd_f(const Inst *__restrict__ insts, const Work *__restrict__ work, int cb)
+__global__ void __launch_bounds__(512, LH_FFT_MINB) k_zfwd_f(const Inst *__restrict__ insts, const Work *__restrict__ work, int cb)
 {
     constexpr int N1 = Plan2<NZ>::N1, N2 = Plan2<NZ>::N2;
     constexpr int Nz = 2 * NZ / 3;

@@ -14,7 +14,7 @@ from dataclasses import dataclass
 import numpy as np
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIBPATH = os.path.join(os.path.dirname(PKG), "build", "liblh_gpu.so")
+LIBPATH = os.environ.get("LH_LIBPATH") or os.path.join(os.path.dirname(PKG), "build", "liblh_gpu.so")
 
 LH_OK, LH_EINVAL, LH_ECUDA, LH_ENOMEM, LH_EDEVICE, LH_ESTATE = 0, -1, -2, -3, -4, -5
 GRID_POLY, GRID_TANH = 0, 1
