@@ -116,13 +116,24 @@ def peaks():
     return 6650.0, "fallback"
 
 
+TRAFFIC_SUMMARY = os.path.join(ROOT, "profiles", "dram_traffic_plain_128x128x153.md")
+
+
 def ncu_traffic():
-    """Per-launch DRAM bytes of the column pass from the committed ncu capture."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(p):
-        with open(p) as f:
-            return json.load(f)
-    return {}
+    """Measured DRAM bytes (read + write) per substep for each kernel class,
+    from the committed ncu summary: lines ``dram_bytes_per_substep[<class>]: N``."""
+    out = {}
+    if os.path.exists(TRAFFIC_SUMMARY):
+        with open(TRAFFIC_SUMMARY) as f:
+            for line in f:
+                line = line.strip().strip("`")
+                if line.startswith("dram_bytes_per_substep[") and "]:" in line:
+                    key, val = line[len("dram_bytes_per_substep["):].split("]:", 1)
+                    try:
+                        out[key] = float(val)
+                    except ValueError:
+                        pass
+    return out
 
 
 def cpu_rate(desc, sample_steps: int, threads: int):
@@ -167,13 +178,24 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def column_alg_bytes(desc):
-    """Algorithmic bytes of one column-pass launch: the 13 fields it must read
-    (u1 u2 u3 p, Nu of the previous substep x3, x/z parts of Nu x3, y-flux
-    spectra x3) and the 7 it must write (u1 u2 u3 p, Nu x3), 16 B per complex
-    entry, ncols x ny entries each."""
-    F = 16 * desc.ncols * desc.ny
-    return 20 * F
+def field_bytes(desc):
+    """F: one complex FP64 field over every column and y row."""
+    return 16 * desc.ncols * desc.ny
+
+
+def substep_alg_bytes(desc):
+    """Algorithmic HBM bytes of one RK3 substep, 20 F: the plane pass reads
+    u1 u2 u3 and writes Nu1 Nu2 Nu3 (6 F); the column pass reads u1 u2 u3 p,
+    the new and the previous Nu (10 F) and writes u1 u2 u3 p (4 F)."""
+    return 20 * field_bytes(desc)
+
+
+# HBM bytes each kernel class of this design moves per substep, in units of
+# F: the z-inverse reads the three velocity planes, the x-products kernel
+# works on the L2-resident staging only, the z-forward writes the x/z parts
+# of Nu and the three y-flux spectra, the column pass reads 13 fields and
+# writes 7 (u1 u2 u3 p, Nu x3).
+DESIGN_F = {"z_inverse": 3, "x_products": 0, "z_forward": 6, "dt": 0, "column": 20}
 
 
 def batched_and_served(args):
@@ -257,12 +279,22 @@ def run_ours(args, rank, world, local_rank):
     prof = e.profile(2)
     launches_per_step = sum(n for _, n in prof.values()) // 2
     dom = max(prof.items(), key=lambda kv: kv[1][0])
-    col_ms, col_n = prof["column"]
-    col_avg_ms = col_ms / col_n
     hbm, src = peaks()
-    alg = column_alg_bytes(desc)
-    achieved = alg / (col_avg_ms * 1e-3) / 1e9
-    traffic = ncu_traffic().get("column_dram_bytes_per_launch")
+    F = field_bytes(desc)
+    alg = substep_alg_bytes(desc)
+    sub_s = ms_max * 1e-3 / (3 * K)  # one substep, from the timed region
+    achieved = alg / sub_s / 1e9
+    traffic = ncu_traffic()
+    traffic_sub = sum(traffic.values()) if traffic else None
+    kernels = {}
+    for name, (kms, kn) in prof.items():
+        per_sub = kms / 6.0  # 2 steps x 3 substeps
+        kb = DESIGN_F[name] * F
+        kernels[name] = {"ms_per_substep": per_sub, "launches_per_substep": kn / 6.0,
+                         "share": kms / sum(v[0] for v in prof.values()),
+                         "design_hbm_bytes_per_substep": kb,
+                         "achieved_gbs": kb / (per_sub * 1e-3) / 1e9 if per_sub > 0 else None,
+                         "ncu_dram_bytes_per_substep": traffic.get(name)}
 
     # end to end through the host-buffer call
     nu, nv, nc = desc.nyu, desc.nyv, desc.ncols
@@ -305,10 +337,12 @@ def run_ours(args, rank, world, local_rank):
             "dtype": "f64", "data": "synthetic", "config": config_dict(desc, world),
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
             "gpu_launches": launches_per_step * K,
-            "roofline": {"bound": "hbm", "kernel": "k_column (column pass)", "achieved": achieved, "peak": hbm,
-                         "peak_source": src, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                         "alg_bytes_per_launch": alg, "avg_launch_ms": col_avg_ms},
-            "kernels_ms_per_step": {k: v[0] / 2 for k, v in prof.items()},
+            "roofline": {"bound": "hbm", "kernel": "one RK3 substep (plane pass k_zinv/k_xprod/k_zfwd + column pass "
+                                                  "k_column), the unit the 20 F algorithmic bytes are counted on",
+                         "achieved": achieved, "peak": hbm, "peak_source": src, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic_sub, "alg_bytes": alg,
+                         "avg_duration_ms": sub_s * 1e3},
+            "kernels": kernels,
             "dominant_kernel": dom[0],
             "cpu_baseline": cpu,
             "batched": batched,
