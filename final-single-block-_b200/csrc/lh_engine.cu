@@ -13,6 +13,20 @@ namespace lh {
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Plane fields (Mz x nxh complex) of the staging buffer for `chunk` planes:
+// the fast path's Sin (chunk + 2 rows x 3 fields) and Sprod (chunk x 6);
+// the generic path uses the first 6 * chunk.
+size_t staging_units(int chunk) { return (size_t)(chunk + 2) * 3 + (size_t)chunk * kNumProducts; }
+
+// Bytes of plane staging one chunk round may use across all instances of a
+// plan, kept well inside the 126 MB L2 (LH_STAGING_MB overrides, for tuning).
+size_t staging_budget()
+{
+    const char *ev = getenv("LH_STAGING_MB");
+    const long mb = ev ? atol(ev) : 0;
+    return (size_t)(mb > 0 ? mb : 96) << 20;
+}
+
 Tiles default_tiles(int Mx, int Mz, int nxh, int nyu)
 {
     Tiles t;
@@ -21,9 +35,11 @@ Tiles default_tiles(int Mx, int Mz, int nxh, int nyu)
     t.br_x = std::max(1, std::min(Mz, (int)(target / (96 * (size_t)Mx))));
     t.bc_zfwd = std::max(1, std::min(nxh, (int)(target / (192 * (size_t)Mz))));
     t.threads = 256;
-    const size_t per_plane = (size_t)kNumProducts * Mz * nxh * sizeof(double2);
-    const size_t budget = 40ull << 20;  // staging kept well inside the 126 MB L2
-    t.chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nyu, budget / per_plane));
+    // staging capacity: the fast path holds 9 plane fields per plane plus 6
+    // for the halo rows (staging_units), the generic path 6 per plane
+    const size_t unit = (size_t)Mz * nxh * sizeof(double2);
+    const size_t units = staging_budget() / unit;
+    t.chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nyu, units > 6 ? (units - 6) / 9 : 1));
     return t;
 }
 
@@ -81,7 +97,7 @@ void carve(const HostSetup &s, int chunk, Carver &c, Inst &I, double2 **stage, s
     I.PSI = c.take<double2>(np * nc);
     I.U11 = c.take<double>(nu);
     I.F11 = c.take<double>(nu);
-    I.S = c.take<double2>((size_t)chunk * kNumProducts * s.Mz * s.nxh);
+    I.S = c.take<double2>(staging_units(chunk) * s.Mz * s.nxh);
     I.sc = c.take<double>(SC_COUNT);
     I.err = c.take<int>(8);
     *stage_elems = nu * nc;
@@ -324,22 +340,24 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
     }
     // Planes per round: the staging of one round, summed over every instance
     // of the plan, stays inside the L2 budget so staging never reaches HBM.
-    const size_t l2_budget = 40ull << 20;
-    std::vector<int> chunk_eff(insts.size());
-    for (size_t q = 0; q < insts.size(); q++) {
-        const HostSetup &s = insts[q]->hs;
-        const size_t per_plane = (size_t)kNumProducts * s.Mz * s.nxh * sizeof(double2);
-        size_t c = l2_budget / (per_plane * insts.size());
-        c = std::max<size_t>(1, std::min<size_t>(c, (size_t)insts[q]->inst.chunk));
-        chunk_eff[q] = (int)c;
-        rounds = std::max(rounds, (s.nyu + chunk_eff[q] - 1) / chunk_eff[q]);
-    }
     const size_t ncls = classes.size();
     std::vector<ClassTiles> tiles(ncls);
     std::vector<const HostSetup *> rep(ncls, nullptr);
     for (size_t q = 0; q < insts.size(); q++)
         if (!rep[cls_of[q]]) rep[cls_of[q]] = &insts[q]->hs;
     for (size_t c = 0; c < ncls; c++) tiles[c] = class_tiles(*rep[c], force_generic);
+    const size_t l2_budget = staging_budget();
+    std::vector<int> chunk_eff(insts.size());
+    for (size_t q = 0; q < insts.size(); q++) {
+        const HostSetup &s = insts[q]->hs;
+        const bool fast = tiles[cls_of[q]].fast;
+        const size_t unit = (size_t)s.Mz * s.nxh * sizeof(double2);
+        const size_t units = l2_budget / (unit * insts.size());
+        size_t c = fast ? (units > 6 ? (units - 6) / 9 : 1) : units / kNumProducts;
+        c = std::max<size_t>(1, std::min<size_t>(c, (size_t)insts[q]->inst.chunk));
+        chunk_eff[q] = (int)c;
+        rounds = std::max(rounds, (s.nyu + chunk_eff[q] - 1) / chunk_eff[q]);
+    }
     // work lists [round][stage][class]
     std::vector<std::vector<std::vector<std::vector<Work>>>> lists(
         rounds, std::vector<std::vector<std::vector<Work>>>(3, std::vector<std::vector<Work>>(ncls)));
@@ -351,13 +369,31 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
         const int nbz = (s.nxh + ct.cbz - 1) / ct.cbz;
         const int nbx = (s.Mz + ct.rbx - 1) / ct.rbx;
         const int nbf = (s.nxh + ct.cbf - 1) / ct.cbf;
-        for (int j = 1; j <= s.nyu; j++) {
-            const int r = (j - 1) / chunk, slot = (j - 1) % chunk;
-            auto &L = lists[r];
-            for (int f = 0; f < kNumProducts; f++)
-                for (int b = 0; b < nbz; b++) L[0][cls_of[q]].push_back({q, j, slot, f * nbz + b});
-            for (int b = 0; b < nbx; b++) L[1][cls_of[q]].push_back({q, j, slot, b});
-            for (int b = 0; b < nbf; b++) L[2][cls_of[q]].push_back({q, j, slot, b});
+        if (ct.fast) {
+            // round r: planes j0..j1; Sin slot p holds y row j0-1+p, u1/u3 on
+            // rows j0..j1+1 and u2 on rows j0-1..j1
+            for (int j0 = 1, r = 0; j0 <= s.nyu; j0 += chunk, r++) {
+                const int j1 = std::min(s.nyu, j0 + chunk - 1);
+                auto &L = lists[r];
+                for (int jp = j0 - 1; jp <= j1 + 1; jp++)
+                    for (int f = 0; f < 3; f++) {
+                        if (f < 2 ? jp < j0 : jp > j1) continue;
+                        for (int b = 0; b < nbz; b++) L[0][cls_of[q]].push_back({q, jp, jp - j0 + 1, f * nbz + b});
+                    }
+                for (int j = j0; j <= j1; j++) {
+                    for (int b = 0; b < nbx; b++) L[1][cls_of[q]].push_back({q, j, j - j0, b});
+                    for (int b = 0; b < nbf; b++) L[2][cls_of[q]].push_back({q, j, j - j0, b});
+                }
+            }
+        } else {
+            for (int j = 1; j <= s.nyu; j++) {
+                const int r = (j - 1) / chunk, slot = (j - 1) % chunk;
+                auto &L = lists[r];
+                for (int f = 0; f < kNumProducts; f++)
+                    for (int b = 0; b < nbz; b++) L[0][cls_of[q]].push_back({q, j, slot, f * nbz + b});
+                for (int b = 0; b < nbx; b++) L[1][cls_of[q]].push_back({q, j, slot, b});
+                for (int b = 0; b < nbf; b++) L[2][cls_of[q]].push_back({q, j, slot, b});
+            }
         }
         for (int b = 0; b < (s.nc + kColumnThreads - 1) / kColumnThreads; b++) p.column.push_back({q, b, 0, 0});
     }
@@ -378,6 +414,7 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
                 g.threads = stg == 0 ? tiles[c].tz : stg == 1 ? tiles[c].tx : tiles[c].tf;
                 g.smem = stg == 0 ? tiles[c].smz : stg == 1 ? tiles[c].smx : tiles[c].smf;
                 g.param = stg == 0 ? tiles[c].cbz : stg == 1 ? tiles[c].rbx : tiles[c].cbf;
+                g.grid = (unsigned)g.count;
                 all.insert(all.end(), v.begin(), v.end());
                 p.rounds[r].push_back(g);
             }
@@ -448,9 +485,11 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
             const unsigned n = (unsigned)g.count;
             time_begin(timer, st);
             if (g.fast) {
-                if (g.stage == 0) fast_launch_zinv(g.Mz, n, g.threads, g.smem, st, d_insts, w, g.param);
-                else if (g.stage == 1) fast_launch_xprod(g.Mx, n, g.threads, g.smem, st, d_insts, w, g.param, want_max);
-                else fast_launch_zfwd(g.Mz, n, g.threads, g.smem, st, d_insts, w, g.param);
+                const int cnt = (int)g.count;
+                if (g.stage == 0) fast_launch_zinv(g.Mz, g.grid, g.threads, g.smem, st, d_insts, w, cnt, g.param);
+                else if (g.stage == 1)
+                    fast_launch_xprod(g.Mx, g.grid, g.threads, g.smem, st, d_insts, w, cnt, g.param, want_max);
+                else fast_launch_zfwd(g.Mz, g.grid, g.threads, g.smem, st, d_insts, w, cnt, g.param);
             } else {
                 if (g.stage == 0) k_zinv<<<n, g.threads, g.smem, st>>>(d_insts, w, g.param);
                 else if (g.stage == 1) k_xprod<<<n, g.threads, g.smem, st>>>(d_insts, w, g.param, want_max);

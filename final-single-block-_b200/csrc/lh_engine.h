@@ -37,6 +37,8 @@ struct DevInstance {
     size_t stage_elems = 0;
 };
 
+// Plane fields of staging an instance allocates for `chunk` planes.
+size_t staging_units(int chunk);
 // Bytes one instance needs for a staging chunk of `chunk` planes.
 size_t instance_bytes(const HostSetup &hs, int chunk);
 // Allocate and fill the device arrays of an instance (synchronous).
@@ -58,6 +60,7 @@ struct Group {
     int threads = 256;
     size_t smem = 0;
     int param = 1;        // cb (z stages) or rb (x stage)
+    unsigned grid = 0;    // CTAs launched, one per work item
 };
 
 // Work tables for a set of instances sharing launches.

@@ -32,10 +32,10 @@ bool fast_size(int n);
 int fast_threads(int n, int vectors);
 cudaError_t fast_set_attributes(int Mz, int Mx, size_t smz, size_t smx, size_t smf);
 void fast_launch_zinv(int Mz, unsigned grid, int threads, size_t smem, cudaStream_t st, const Inst *insts,
-                      const Work *work, int cb);
+                      const Work *work, int count, int cb);
 void fast_launch_xprod(int Mx, unsigned grid, int threads, size_t smem, cudaStream_t st, const Inst *insts,
-                       const Work *work, int rb, int want_max);
+                       const Work *work, int count, int rb, int want_max);
 void fast_launch_zfwd(int Mz, unsigned grid, int threads, size_t smem, cudaStream_t st, const Inst *insts,
-                      const Work *work, int cb);
+                      const Work *work, int count, int cb);
 
 }  // namespace lh
