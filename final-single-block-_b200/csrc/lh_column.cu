@@ -54,8 +54,10 @@ __device__ __forceinline__ double2 cscale(double s, double2 a) { return make_dou
 // a warp touch 512 contiguous bytes.
 constexpr int kColThreads = kColumnThreads;
 constexpr int kRoles = kColumnBlock / kColumnThreads;
-constexpr int kStages = 8;
-constexpr int kSlots = 5;
+// Row slots (one complex per lane, 512 B per warp) of shared memory each
+// warp owns; a phase that loads S slots per row keeps kWarpSlots / S rows in
+// flight, and the single-warp Poisson sweeps use all warps' slots.
+constexpr int kWarpSlots = 40;
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void cp16(double2 *s, const double2 *g)
@@ -73,30 +75,43 @@ __device__ __forceinline__ void cp_wait()
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// Per-thread ring of kStages row stages with kSlots complex slots each,
-// laid out [stage][slot][lane] so a warp's 32 lanes touch 512 contiguous
-// bytes; every warp of the CTA owns one ring.
+// Ring of D row stages with S complex slots each, laid out
+// [stage][slot][lane] so a warp's 32 lanes touch 512 contiguous bytes.
+template <int D, int S>
 struct Ring {
+    static constexpr int kDepth = D;
     double2 *base;
     int lane;
-    __device__ double2 *at(int stage, int slot) const { return base + ((stage * kSlots + slot) * kColThreads + lane); }
+    __device__ double2 *at(int stage, int slot) const { return base + ((stage * S + slot) * kColThreads + lane); }
 };
 
-size_t column_smem_bytes() { return (size_t)kRoles * kStages * kSlots * kColThreads * sizeof(double2); }
+// Doubles of the per-row y metrics staged in shared memory: d2/dy2
+// coefficients of both grids, dtheta/dy of both grids, DG1.
+__host__ __device__ inline size_t column_metric_doubles(int nyu, int nyv)
+{
+    return 4 * (size_t)(nyu + 2) + 4 * (size_t)(nyv + 2) + (size_t)(nyu + 1);
+}
 
-// Row streamer: rows are visited in order r = 0..n-1; fill(r, stage) issues
-// the copies of row r.  Keeps kStages-1 rows in flight.
-template <class Fill, class Use>
+size_t column_smem_bytes(int max_nyu)
+{
+    return (size_t)kRoles * kWarpSlots * kColThreads * sizeof(double2) +
+           column_metric_doubles(max_nyu, max_nyu - 1) * sizeof(double);
+}
+
+// Row streamer over a ring of depth D: rows are visited in order
+// r = 0..n-1; fill(r, stage) issues the copies of row r.  Keeps D-1 rows in
+// flight.
+template <int D, class Fill, class Use>
 __device__ __forceinline__ void stream_rows(int n, Fill &&fill, Use &&use)
 {
-    for (int r = 0; r < kStages - 1; r++) {
-        if (r < n) fill(r, r % kStages);
+    for (int r = 0; r < D - 1; r++) {
+        if (r < n) fill(r, r % D);
         cp_commit();
     }
     for (int r = 0; r < n; r++) {
-        cp_wait<kStages - 2>();
-        use(r, r % kStages);
-        if (r + kStages - 1 < n) fill(r + kStages - 1, (r + kStages - 1) % kStages);
+        cp_wait<D - 2>();
+        use(r, r % D);
+        if (r + D - 1 < n) fill(r + D - 1, (r + D - 1) % D);
         cp_commit();
     }
     cp_wait<0>();
@@ -126,8 +141,21 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
     double2 *U1 = I.U1 + cc, *U2 = I.U2 + cc, *U3 = I.U3 + cc, *P = I.P + cc;
     double2 *PS = I.PSI + cc;
     double *FU = I.FACU + cc, *FV = I.FACV + cc;
-    const double *du = I.dyu2i, *dv = I.dyv2i;
-    Ring ring{ring_mem + (size_t)role * kStages * kSlots * kColThreads, lane};
+    // per-row y metrics, read by every row of every sweep, staged once
+    double *sdu = reinterpret_cast<double *>(ring_mem + (size_t)kRoles * kWarpSlots * kColThreads);
+    double *sdv = sdu + 3 * (nyu + 2), *sthu = sdv + 3 * (nyv + 2), *sthv = sthu + (nyu + 2), *sdg1 = sthv + (nyv + 2);
+    for (int e = threadIdx.x; e < 3 * (nyu + 2); e += blockDim.x) sdu[e] = I.dyu2i[e];
+    for (int e = threadIdx.x; e < 3 * (nyv + 2); e += blockDim.x) sdv[e] = I.dyv2i[e];
+    for (int e = threadIdx.x; e < nyu + 2; e += blockDim.x) sthu[e] = I.dthdyu[e];
+    for (int e = threadIdx.x; e < nyv + 2; e += blockDim.x) sthv[e] = I.dthdyv[e];
+    for (int e = threadIdx.x; e < nyu + 1; e += blockDim.x) sdg1[e] = I.DG1[e];
+    __syncthreads();
+    const double *du = sdu, *dv = sdv;
+    double2 *warp_mem = ring_mem + (size_t)role * kWarpSlots * kColThreads;
+    using RingA = Ring<kWarpSlots / 5, 5>;         // phase A: 5 slots per row
+    using RingW2 = Ring<kWarpSlots / 2, 2>;        // phases B, D2: 2 slots per row
+    using RingC = Ring<kRoles * kWarpSlots / 4, 4>;   // phase C (u1 warp, all slots)
+    using RingD = Ring<kRoles * kWarpSlots / 3, 3>;   // phase D1 (u1 warp, all slots)
 
     // ---------------- A: right-hand sides and forward elimination --------
     if (live && role < 2) {
@@ -148,7 +176,8 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
         double2 yp = make_double2(0.0, 0.0);
         U[0] = yp;
         if (role == 0) FU[0] = a3u;
-        stream_rows(nyu,
+        const RingA ring{warp_mem, lane};
+        stream_rows<RingA::kDepth>(nyu,
                     [&](int r, int st) {
                         const int j = r + 1;
                         const size_t o = (size_t)j * nc, on = o - nc;
@@ -168,7 +197,7 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         const double2 L = make_double2(d1 * um.x + cen * uc.x + d3 * up.x, d1 * um.y + cen * uc.y + d3 * up.y);
                         double2 dd = make_double2(C1 * L.x + C2 * no.x + dC3 * pj.y, C1 * L.y + C2 * no.y + -(dC3 * pj.x));
                         if (role == 0 && mean) dd.x = dd.x + C1m;
-                        const double m = I.dthdyu[j];
+                        const double m = sthu[j];
                         const double2 nu = make_double2(x.x + (fl.x - flp.x) * m * ddv, x.y + (fl.y - flp.y) * m * ddv);
                         N[on] = nu;
                         dd = make_double2(dd.x + G * nu.x, dd.y + G * nu.y);
@@ -202,7 +231,8 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
         double2 yp = make_double2(0.0, 0.0);
         U2[0] = yp;
         FV[0] = a3v;
-        stream_rows(nyv,
+        const RingA ring{warp_mem, lane};
+        stream_rows<RingA::kDepth>(nyv,
                     [&](int r, int st) {
                         const int j = r + 1;
                         const size_t o = (size_t)j * nc, on = o - nc;
@@ -220,7 +250,7 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         const double e1 = dv[3 * j], e2 = dv[3 * j + 1], e3 = dv[3 * j + 2];
                         const double cenv = k2x + k2z + e2;
                         const double2 L = make_double2(e1 * um.x + cenv * uc.x + e3 * up.x, e1 * um.y + cenv * uc.y + e3 * up.y);
-                        const double mv = I.dthdyv[j];
+                        const double mv = sthv[j];
                         const double C3 = -rk.d * ddv * mv;
                         double2 dd = make_double2(C1 * L.x + C2 * no.x + C3 * (pn.x - pc.x), C1 * L.y + C2 * no.y + C3 * (pn.y - pc.y));
                         const double2 nu = make_double2(x.x + (vvn.x - vvc.x) * mv * ddv, x.y + (vvn.y - vvc.y) * mv * ddv);
@@ -252,7 +282,8 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
         const double *F = role == 2 ? FV : FU;
         const int top = role == 2 ? nyv + 1 : nyu + 1;
         double2 v = U[(size_t)top * nc];
-        stream_rows(top,
+        const RingW2 ring{warp_mem, lane};
+        stream_rows<RingW2::kDepth>(top,
                     [&](int r, int st) {
                         const int j = top - 1 - r;
                         cp16(ring.at(st, 0), U + (size_t)j * nc);
@@ -324,7 +355,8 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
         const double *G2 = I.DG2 + cc;
         double2 v2m = U2[0];
         double2 xp = make_double2(0.0, 0.0);
-        stream_rows(nyu,
+        const RingC ring{ring_mem, lane};
+        stream_rows<RingC::kDepth>(nyu,
                     [&](int r, int st) {
                         const int j = r + 1;
                         const size_t o = (size_t)j * nc;
@@ -337,7 +369,7 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         const int j = r + 1;
                         const double2 a = *ring.at(st, 0), c3 = *ring.at(st, 1), v2c = *ring.at(st, 2);
                         const double g2 = ring.at(st, 3)->x;
-                        const double mm = ddv * I.dthdyu[j];
+                        const double mm = ddv * sthu[j];
                         const double2 d = make_double2(-(kxr * a.y) + -(kzr * c3.y) + mm * (v2c.x - v2m.x),
                                                        kxr * a.x + kzr * c3.x + mm * (v2c.y - v2m.y));
                         double2 ps = cscale(dtirk, d);
@@ -345,7 +377,7 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         if (j == 1) {
                             xp = cscale(g2, ps);
                         } else {
-                            const double g1 = I.DG1[j];
+                            const double g1 = sdg1[j];
                             xp = make_double2((ps.x - g1 * xp.x) * g2, (ps.y - g1 * xp.y) * g2);
                         }
                         PS[(size_t)(j - 1) * nc] = xp;
@@ -355,21 +387,22 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
         // ---------------- D1: LUsolP back sweep and p += psi ---------------
         const double *G3 = I.DG3 + cc;
         double2 psn = xp;  // psi(nyu) = x(nyu)
-        stream_rows(nyu,
+        const RingD ringd{ring_mem, lane};
+        stream_rows<RingD::kDepth>(nyu,
                     [&](int r, int st) {
                         const int j = nyu - r;
                         const size_t o = (size_t)(j - 1) * nc;
-                        cp16(ring.at(st, 0), PS + o);
-                        cp16(ring.at(st, 1), P + o);
-                        if (j < nyu) cp8(&ring.at(st, 2)->x, G3 + o);
+                        cp16(ringd.at(st, 0), PS + o);
+                        cp16(ringd.at(st, 1), P + o);
+                        if (j < nyu) cp8(&ringd.at(st, 2)->x, G3 + o);
                     },
                     [&](int r, int st) {
                         const int j = nyu - r;
                         const size_t o = (size_t)(j - 1) * nc;
-                        const double2 x = *ring.at(st, 0), p = *ring.at(st, 1);
+                        const double2 x = *ringd.at(st, 0), p = *ringd.at(st, 1);
                         double2 ps = x;
                         if (j < nyu) {
-                            const double g3 = ring.at(st, 2)->x;
+                            const double g3 = ringd.at(st, 2)->x;
                             ps = make_double2(x.x - g3 * psn.x, x.y - g3 * psn.y);
                         }
                         PS[o] = ps;
@@ -385,7 +418,8 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
         double2 *U = role == 0 ? U1 : U3;
         const double kd = dtrk * (role == 0 ? kxr : kzr);
         double2 first = make_double2(0.0, 0.0), last = first, ps1 = first;
-        stream_rows(nyu,
+        const RingW2 ring{warp_mem, lane};
+        stream_rows<RingW2::kDepth>(nyu,
                     [&](int r, int st) {
                         const int j = r + 1;
                         cp16(ring.at(st, 0), U + (size_t)j * nc);
@@ -418,7 +452,8 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
     } else if (live && role == 2) {
         const double dtrk_u2 = dtrk * ddv;
         double2 psc = PS[0];  // psi(j) of the current row
-        stream_rows(nyv,
+        const RingW2 ring{warp_mem, lane};
+        stream_rows<RingW2::kDepth>(nyv,
                     [&](int r, int st) {
                         const int j = r + 1;
                         cp16(ring.at(st, 0), U2 + (size_t)j * nc);
@@ -428,7 +463,7 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         const int j = r + 1;
                         double2 v = *ring.at(st, 0);
                         const double2 psn = *ring.at(st, 1);
-                        const double mv = dtrk_u2 * I.dthdyv[j];
+                        const double mv = dtrk_u2 * sthv[j];
                         v = make_double2(v.x - mv * (psn.x - psc.x), v.y - mv * (psn.y - psc.y));
                         U2[(size_t)j * nc] = v;
                         psc = psn;

@@ -446,7 +446,9 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
         return e;
     if (gf && (e = cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gf)) != cudaSuccess)
         return e;
-    p.sm_col = column_smem_bytes();
+    int max_nyu = 1;
+    for (const DevInstance *d : insts) max_nyu = std::max(max_nyu, d->hs.nyu);
+    p.sm_col = column_smem_bytes(max_nyu);
     return cudaFuncSetAttribute(k_column, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.sm_col);
 }
 

@@ -7,7 +7,7 @@ namespace lh {
 
 constexpr int kColumnThreads = 32;       // columns per column-pass CTA (one lane each)
 constexpr int kColumnBlock = 3 * kColumnThreads;  // three warps: the u1, u3 and u2 chains
-size_t column_smem_bytes();
+size_t column_smem_bytes(int max_nyu);  // ring + staged y metrics
 
 __global__ void k_zinv(const Inst *__restrict__ insts, const Work *__restrict__ work, int bc);
 __global__ void k_xprod(const Inst *__restrict__ insts, const Work *__restrict__ work, int br, int want_max);
