@@ -68,11 +68,11 @@ __device__ __forceinline__ void cp8(double *s, const double *g)
 {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(s)), "l"(g));
 }
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait()
 {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // Ring of D row stages with S complex slots each, laid out
@@ -99,23 +99,65 @@ size_t column_smem_bytes(int max_nyu)
 }
 
 // Row streamer over a ring of depth D: rows are visited in order
-// r = 0..n-1; fill(r, stage) issues the copies of row r.  Keeps D-1 rows in
-// flight.
-template <int D, class Fill, class Use>
-__device__ __forceinline__ void stream_rows(int n, Fill &&fill, Use &&use)
+// r = 0..n-1.  fill(r, stage) issues the copies of row r; load(r, stage)
+// reads the landed row (and its shared-memory metrics) into registers;
+// use(r, row) consumes it.  Keeps D-1 rows in flight and handles U rows per
+// step, all loads first, so the reads of the next rows are not ordered
+// behind the global stores of the current one and overlap its recurrence.
+template <int D, int U, class Fill, class Load, class Use>
+__device__ __forceinline__ void stream_rows(int n, Fill &&fill, Load &&load, Use &&use)
 {
+    static_assert(U >= 1 && U < D - 1, "unroll must leave rows in flight");
+    using Row = decltype(load(0, 0));
     for (int r = 0; r < D - 1; r++) {
         if (r < n) fill(r, r % D);
         cp_commit();
     }
-    for (int r = 0; r < n; r++) {
+    int r = 0;
+    for (; r + U <= n; r += U) {
+        cp_wait<D - 1 - U>();  // rows r .. r+U-1 have landed
+        Row v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) v[u] = load(r + u, (r + u) % D);
+#pragma unroll
+        for (int u = 0; u < U; u++) use(r + u, v[u]);
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int rn = r + D - 1 + u;  // reuses the stage of row r-1+u
+            if (rn < n) fill(rn, rn % D);
+            cp_commit();
+        }
+    }
+    for (; r < n; r++) {
         cp_wait<D - 2>();
-        use(r, r % D);
+        const Row v = load(r, r % D);
+        use(r, v);
         if (r + D - 1 < n) fill(r + D - 1, (r + D - 1) % D);
         cp_commit();
     }
     cp_wait<0>();
 }
+
+struct RowA {
+    double2 a, b, c, d, e;
+    double m0, m1, m2, m3;
+};
+struct RowB {
+    double2 y;
+    double f;
+};
+struct RowC {
+    double2 a, c3, v2c;
+    double g2, th, g1;
+};
+struct RowD {
+    double2 x, p;
+    double g3;
+};
+struct RowE {
+    double2 a, ps;
+    double th;
+};
 
 __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__restrict__ insts,
                                                                 const Work *__restrict__ work, int kRK)
@@ -177,7 +219,7 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
         U[0] = yp;
         if (role == 0) FU[0] = a3u;
         const RingA ring{warp_mem, lane};
-        stream_rows<RingA::kDepth>(nyu,
+        stream_rows<RingA::kDepth, 2>(nyu,
                     [&](int r, int st) {
                         const int j = r + 1;
                         const size_t o = (size_t)j * nc, on = o - nc;
@@ -189,15 +231,19 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                     },
                     [&](int r, int st) {
                         const int j = r + 1;
+                        return RowA{*ring.at(st, 0), *ring.at(st, 1), *ring.at(st, 2), *ring.at(st, 3), *ring.at(st, 4),
+                                    du[3 * j], du[3 * j + 1], du[3 * j + 2], sthu[j]};
+                    },
+                    [&](int r, const RowA &w) {
+                        const int j = r + 1;
                         const size_t o = (size_t)j * nc, on = o - nc;
-                        const double2 up = *ring.at(st, 0), pj = *ring.at(st, 1), no = *ring.at(st, 2);
-                        const double2 x = *ring.at(st, 3), fl = *ring.at(st, 4);
-                        const double d1 = du[3 * j], d2 = du[3 * j + 1], d3 = du[3 * j + 2];
+                        const double2 up = w.a, pj = w.b, no = w.c, x = w.d, fl = w.e;
+                        const double d1 = w.m0, d2 = w.m1, d3 = w.m2;
                         const double cen = k2x + k2z + d2;
                         const double2 L = make_double2(d1 * um.x + cen * uc.x + d3 * up.x, d1 * um.y + cen * uc.y + d3 * up.y);
                         double2 dd = make_double2(C1 * L.x + C2 * no.x + dC3 * pj.y, C1 * L.y + C2 * no.y + -(dC3 * pj.x));
                         if (role == 0 && mean) dd.x = dd.x + C1m;
-                        const double m = sthu[j];
+                        const double m = w.m3;
                         const double2 nu = make_double2(x.x + (fl.x - flp.x) * m * ddv, x.y + (fl.y - flp.y) * m * ddv);
                         N[on] = nu;
                         dd = make_double2(dd.x + G * nu.x, dd.y + G * nu.y);
@@ -232,7 +278,7 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
         U2[0] = yp;
         FV[0] = a3v;
         const RingA ring{warp_mem, lane};
-        stream_rows<RingA::kDepth>(nyv,
+        stream_rows<RingA::kDepth, 2>(nyv,
                     [&](int r, int st) {
                         const int j = r + 1;
                         const size_t o = (size_t)j * nc, on = o - nc;
@@ -244,13 +290,17 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                     },
                     [&](int r, int st) {
                         const int j = r + 1;
+                        return RowA{*ring.at(st, 0), *ring.at(st, 1), *ring.at(st, 2), *ring.at(st, 3), *ring.at(st, 4),
+                                    dv[3 * j], dv[3 * j + 1], dv[3 * j + 2], sthv[j]};
+                    },
+                    [&](int r, const RowA &w) {
+                        const int j = r + 1;
                         const size_t o = (size_t)j * nc, on = o - nc;
-                        const double2 up = *ring.at(st, 0), pn = *ring.at(st, 1), no = *ring.at(st, 2);
-                        const double2 x = *ring.at(st, 3), vvn = *ring.at(st, 4);
-                        const double e1 = dv[3 * j], e2 = dv[3 * j + 1], e3 = dv[3 * j + 2];
+                        const double2 up = w.a, pn = w.b, no = w.c, x = w.d, vvn = w.e;
+                        const double e1 = w.m0, e2 = w.m1, e3 = w.m2;
                         const double cenv = k2x + k2z + e2;
                         const double2 L = make_double2(e1 * um.x + cenv * uc.x + e3 * up.x, e1 * um.y + cenv * uc.y + e3 * up.y);
-                        const double mv = sthv[j];
+                        const double mv = w.m3;
                         const double C3 = -rk.d * ddv * mv;
                         double2 dd = make_double2(C1 * L.x + C2 * no.x + C3 * (pn.x - pc.x), C1 * L.y + C2 * no.y + C3 * (pn.y - pc.y));
                         const double2 nu = make_double2(x.x + (vvn.x - vvc.x) * mv * ddv, x.y + (vvn.y - vvc.y) * mv * ddv);
@@ -283,16 +333,17 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
         const int top = role == 2 ? nyv + 1 : nyu + 1;
         double2 v = U[(size_t)top * nc];
         const RingW2 ring{warp_mem, lane};
-        stream_rows<RingW2::kDepth>(top,
+        stream_rows<RingW2::kDepth, 4>(top,
                     [&](int r, int st) {
                         const int j = top - 1 - r;
                         cp16(ring.at(st, 0), U + (size_t)j * nc);
                         cp8(&ring.at(st, 1)->x, F + (size_t)j * nc);
                     },
-                    [&](int r, int st) {
+                    [&](int r, int st) { return RowB{*ring.at(st, 0), ring.at(st, 1)->x}; },
+                    [&](int r, const RowB &w) {
                         const int j = top - 1 - r;
-                        const double2 y = *ring.at(st, 0);
-                        const double f = ring.at(st, 1)->x;
+                        const double2 y = w.y;
+                        const double f = w.f;
                         v = make_double2(y.x - f * v.x, y.y - f * v.y);
                         U[(size_t)j * nc] = v;
                     });
@@ -356,7 +407,7 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
         double2 v2m = U2[0];
         double2 xp = make_double2(0.0, 0.0);
         const RingC ring{ring_mem, lane};
-        stream_rows<RingC::kDepth>(nyu,
+        stream_rows<RingC::kDepth, 4>(nyu,
                     [&](int r, int st) {
                         const int j = r + 1;
                         const size_t o = (size_t)j * nc;
@@ -367,9 +418,13 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                     },
                     [&](int r, int st) {
                         const int j = r + 1;
-                        const double2 a = *ring.at(st, 0), c3 = *ring.at(st, 1), v2c = *ring.at(st, 2);
-                        const double g2 = ring.at(st, 3)->x;
-                        const double mm = ddv * sthu[j];
+                        return RowC{*ring.at(st, 0), *ring.at(st, 1), *ring.at(st, 2), ring.at(st, 3)->x, sthu[j], sdg1[j]};
+                    },
+                    [&](int r, const RowC &w) {
+                        const int j = r + 1;
+                        const double2 a = w.a, c3 = w.c3, v2c = w.v2c;
+                        const double g2 = w.g2;
+                        const double mm = ddv * w.th;
                         const double2 d = make_double2(-(kxr * a.y) + -(kzr * c3.y) + mm * (v2c.x - v2m.x),
                                                        kxr * a.x + kzr * c3.x + mm * (v2c.y - v2m.y));
                         double2 ps = cscale(dtirk, d);
@@ -377,18 +432,17 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         if (j == 1) {
                             xp = cscale(g2, ps);
                         } else {
-                            const double g1 = sdg1[j];
+                            const double g1 = w.g1;
                             xp = make_double2((ps.x - g1 * xp.x) * g2, (ps.y - g1 * xp.y) * g2);
                         }
                         PS[(size_t)(j - 1) * nc] = xp;
                         v2m = v2c;
                     });
-        __threadfence_block();
         // ---------------- D1: LUsolP back sweep and p += psi ---------------
         const double *G3 = I.DG3 + cc;
         double2 psn = xp;  // psi(nyu) = x(nyu)
         const RingD ringd{ring_mem, lane};
-        stream_rows<RingD::kDepth>(nyu,
+        stream_rows<RingD::kDepth, 4>(nyu,
                     [&](int r, int st) {
                         const int j = nyu - r;
                         const size_t o = (size_t)(j - 1) * nc;
@@ -398,15 +452,15 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                     },
                     [&](int r, int st) {
                         const int j = nyu - r;
+                        return RowD{*ringd.at(st, 0), *ringd.at(st, 1), j < nyu ? ringd.at(st, 2)->x : 0.0};
+                    },
+                    [&](int r, const RowD &w) {
+                        const int j = nyu - r;
                         const size_t o = (size_t)(j - 1) * nc;
-                        const double2 x = *ringd.at(st, 0), p = *ringd.at(st, 1);
-                        double2 ps = x;
-                        if (j < nyu) {
-                            const double g3 = ringd.at(st, 2)->x;
-                            ps = make_double2(x.x - g3 * psn.x, x.y - g3 * psn.y);
-                        }
+                        double2 ps = w.x;
+                        if (j < nyu) ps = make_double2(w.x.x - w.g3 * psn.x, w.x.y - w.g3 * psn.y);
                         PS[o] = ps;
-                        P[o] = make_double2(p.x + ps.x, p.y + ps.y);
+                        P[o] = make_double2(w.p.x + ps.x, w.p.y + ps.y);
                         psn = ps;
                     });
     }
@@ -419,16 +473,17 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
         const double kd = dtrk * (role == 0 ? kxr : kzr);
         double2 first = make_double2(0.0, 0.0), last = first, ps1 = first;
         const RingW2 ring{warp_mem, lane};
-        stream_rows<RingW2::kDepth>(nyu,
+        stream_rows<RingW2::kDepth, 4>(nyu,
                     [&](int r, int st) {
                         const int j = r + 1;
                         cp16(ring.at(st, 0), U + (size_t)j * nc);
                         cp16(ring.at(st, 1), PS + (size_t)(j - 1) * nc);
                     },
-                    [&](int r, int st) {
+                    [&](int r, int st) { return RowE{*ring.at(st, 0), *ring.at(st, 1), 0.0}; },
+                    [&](int r, const RowE &w) {
                         const int j = r + 1;
-                        double2 a = *ring.at(st, 0);
-                        const double2 ps = *ring.at(st, 1);
+                        double2 a = w.a;
+                        const double2 ps = w.ps;
                         a = make_double2(a.x - -(kd * ps.y), a.y - kd * ps.x);
                         U[(size_t)j * nc] = a;
                         if (j == 1) {
@@ -453,17 +508,18 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
         const double dtrk_u2 = dtrk * ddv;
         double2 psc = PS[0];  // psi(j) of the current row
         const RingW2 ring{warp_mem, lane};
-        stream_rows<RingW2::kDepth>(nyv,
+        stream_rows<RingW2::kDepth, 4>(nyv,
                     [&](int r, int st) {
                         const int j = r + 1;
                         cp16(ring.at(st, 0), U2 + (size_t)j * nc);
                         cp16(ring.at(st, 1), PS + (size_t)j * nc);  // psi(j+1)
                     },
-                    [&](int r, int st) {
+                    [&](int r, int st) { return RowE{*ring.at(st, 0), *ring.at(st, 1), sthv[r + 1]}; },
+                    [&](int r, const RowE &w) {
                         const int j = r + 1;
-                        double2 v = *ring.at(st, 0);
-                        const double2 psn = *ring.at(st, 1);
-                        const double mv = dtrk_u2 * sthv[j];
+                        double2 v = w.a;
+                        const double2 psn = w.ps;
+                        const double mv = dtrk_u2 * w.th;
                         v = make_double2(v.x - mv * (psn.x - psc.x), v.y - mv * (psn.y - psc.y));
                         U2[(size_t)j * nc] = v;
                         psc = psn;

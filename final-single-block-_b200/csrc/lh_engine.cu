@@ -257,17 +257,31 @@ struct ClassTiles {
     size_t smz, smx, smf;
 };
 
+// Fast-path launch shapes from upper bounds on the x modes per z-inverse
+// CTA, the z rows per x CTA and the x modes per z-forward CTA; every bound is
+// lowered until the block fits the kernel's launch bounds and 110 KB of
+// shared memory, and the x-mode blocks are balanced.
 ClassTiles fast_tiles(const HostSetup &s, int cbz_max, int rb, int cbf_max)
 {
     ClassTiles c{};
     c.fast = true;
+    const size_t smax = 110 * 1024;
+    auto fits = [&](int stage, int M, int vectors, int per) {
+        return fast_threads(M, vectors) <= fast_max_threads(stage) && (size_t)M * (1 + per) * 16 <= smax;
+    };
+    cbz_max = std::max(1, std::min(cbz_max, s.nxh));
+    while (cbz_max > 1 && !fits(0, s.Mz, cbz_max, cbz_max)) cbz_max--;
     int nb = (s.nxh + cbz_max - 1) / cbz_max;
     c.cbz = (s.nxh + nb - 1) / nb;
     c.tz = fast_threads(s.Mz, c.cbz);
     c.smz = (size_t)s.Mz * (1 + c.cbz) * sizeof(double2);
+    rb = std::max(1, std::min(rb, s.Mz));
+    while (rb > 1 && !fits(1, s.Mx, 3 * rb, 3 * rb)) rb--;
     c.rbx = rb;
     c.tx = fast_threads(s.Mx, 3 * rb);
     c.smx = (size_t)s.Mx * (1 + 3 * rb) * sizeof(double2);
+    cbf_max = std::max(1, std::min(cbf_max, s.nxh));
+    while (cbf_max > 1 && !fits(2, s.Mz, 6 * cbf_max, 6 * cbf_max)) cbf_max--;
     nb = (s.nxh + cbf_max - 1) / cbf_max;
     c.cbf = (s.nxh + nb - 1) / nb;
     c.tf = fast_threads(s.Mz, 6 * c.cbf);
@@ -283,28 +297,9 @@ ClassTiles class_tiles(const HostSetup &s, bool force_generic)
     int a = 0, b = 0, d = 0;
     if (c.fast && ov && sscanf(ov, "%d,%d,%d", &a, &b, &d) == 3 && a > 0 && b > 0 && d > 0) return fast_tiles(s, a, b, d);
     if (c.fast) {
-        const int mz = fast_threads(s.Mz, 1), mx = fast_threads(s.Mx, 1);  // max(N1,N2) rounded to 32
-        (void)mz;
-        (void)mx;
-        // z inverse: up to 16 x modes per CTA, balanced blocks
-        int nb = (s.nxh + 15) / 16;
-        c.cbz = (s.nxh + nb - 1) / nb;
-        c.tz = fast_threads(s.Mz, c.cbz);
-        c.smz = (size_t)s.Mz * (1 + c.cbz) * sizeof(double2);
-        // x products: 3 rb vectors, <= 512 threads, <= 110 KB
-        int rb = 8;
-        while (rb > 1 && (fast_threads(s.Mx, 3 * rb) > 512 || (size_t)s.Mx * (1 + 3 * rb) * 16 > 110 * 1024)) rb--;
-        c.rbx = rb;
-        c.tx = fast_threads(s.Mx, 3 * rb);
-        c.smx = (size_t)s.Mx * (1 + 3 * rb) * sizeof(double2);
-        // z forward: 6 cb vectors, <= 512 threads, <= 110 KB
-        int cbmax = 8;
-        while (cbmax > 1 && (fast_threads(s.Mz, 6 * cbmax) > 512 || (size_t)s.Mz * (1 + 6 * cbmax) * 16 > 110 * 1024))
-            cbmax--;
-        nb = (s.nxh + cbmax - 1) / cbmax;
-        c.cbf = (s.nxh + nb - 1) / nb;
-        c.tf = fast_threads(s.Mz, 6 * c.cbf);
-        c.smf = (size_t)s.Mz * (1 + 6 * c.cbf) * sizeof(double2);
+        // measured on B200 at 128^2 and 32^2: 16 x modes per z-inverse CTA,
+        // 4 z rows per x CTA, up to 8 x modes per z-forward CTA
+        c = fast_tiles(s, 16, 4, 8);
     } else {
         Tiles t = default_tiles(s.Mx, s.Mz, s.nxh, s.nyu);
         c.cbz = t.bc_zinv;

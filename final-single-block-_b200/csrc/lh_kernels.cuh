@@ -30,6 +30,7 @@ __global__ void k_divmax(const Inst *__restrict__ insts, double *out);
 // compile-time-sized fast path (lh_plane_fast.cu)
 bool fast_size(int n);
 int fast_threads(int n, int vectors);
+int fast_max_threads(int stage);  // launch-bounds block size of a fast stage
 cudaError_t fast_set_attributes(int Mz, int Mx, size_t smz, size_t smx, size_t smf);
 void fast_launch_zinv(int Mz, unsigned grid, int threads, size_t smem, cudaStream_t st, const Inst *insts,
                       const Work *work, int count, int cb);

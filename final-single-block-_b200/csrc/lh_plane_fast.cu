@@ -17,9 +17,28 @@
 // fields per plane instead of six.
 #include "lh_fft.cuh"
 
-// resident CTAs per SM the register allocation is sized for
+// Launch bounds (max threads, min resident CTAs per SM) each kernel's
+// register allocation is sized for.
 #ifndef LH_FFT_MINB
 #define LH_FFT_MINB 2
+#endif
+#ifndef LH_ZINV_T
+#define LH_ZINV_T 256
+#endif
+#ifndef LH_ZINV_B
+#define LH_ZINV_B 3
+#endif
+#ifndef LH_XPROD_T
+#define LH_XPROD_T 256
+#endif
+#ifndef LH_XPROD_B
+#define LH_XPROD_B 3
+#endif
+#ifndef LH_ZFWD_T
+#define LH_ZFWD_T 512
+#endif
+#ifndef LH_ZFWD_B
+#define LH_ZFWD_B LH_FFT_MINB
 #endif
 #include "lh_kernels.cuh"
 
@@ -38,7 +57,7 @@ __device__ __forceinline__ double2 *sprod_slot(const Inst &I, int s)
 // z inverse of one (y row jp, field f in {u1, u3, u2}, block of cb x modes):
 // the pruned cft of four_to_phys_u (FOU3D.f90:653-679), -> Sin[slot][f]
 template <int NZ>
-__global__ void __launch_bounds__(512, LH_FFT_MINB) k_zinv_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
+__global__ void __launch_bounds__(LH_ZINV_T, LH_ZINV_B) k_zinv_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
                                                          int count, int cb)
 {
     constexpr int N1 = Plan2<NZ>::N1, N2 = Plan2<NZ>::N2;
@@ -98,7 +117,7 @@ __global__ void __launch_bounds__(512, LH_FFT_MINB) k_zinv_f(const Inst *__restr
 // complex FFT), products, forward real x FFT (ops_in_planes2,
 // FOU3D.f90:1514-1652) -> Sprod[slot]
 template <int NX>
-__global__ void __launch_bounds__(512, LH_FFT_MINB) k_xprod_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
+__global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
                                                           int count, int rb, int want_max)
 {
     constexpr int N1 = Plan2<NX>::N1, N2 = Plan2<NX>::N2;
@@ -290,7 +309,7 @@ __global__ void __launch_bounds__(512, LH_FFT_MINB) k_xprod_f(const Inst *__rest
 // phys_to_four_du's cft (FOU3D.f90:1654-1672), der_x/der_z (:420-523) and
 // planes_to_modes_UVP/NUVP -> NXZ1..3, UVF, WVF, VVC
 template <int NZ>
-__global__ void __launch_bounds__(512, LH_FFT_MINB) k_zfwd_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
+__global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
                                                          int count, int cb)
 {
     constexpr int N1 = Plan2<NZ>::N1, N2 = Plan2<NZ>::N2;
@@ -367,6 +386,8 @@ __global__ void __launch_bounds__(512, LH_FFT_MINB) k_zfwd_f(const Inst *__restr
 
 // ---------------------------------------------------------------------------
 // host dispatch
+int fast_max_threads(int stage) { return stage == 0 ? LH_ZINV_T : (stage == 1 ? LH_XPROD_T : LH_ZFWD_T); }
+
 bool fast_size(int n)
 {
     switch (n) {

@@ -215,10 +215,13 @@ def test_step_host_matches_device_path():
         assert np.array_equal(b, ref[f]), f
 
 
-@pytest.mark.parametrize("N", [32, 64])
+@pytest.mark.parametrize("N", [32, 64, 128, 192, 256])
 def test_fast_and_generic_fft_paths_agree(N, monkeypatch):
     """The compile-time-sized plane kernels and the generic ones give the
-    same step to round-off (both are checked against the oracle above)."""
+    same step to round-off (both are checked against the oracle above), at
+    every Ngal size of the fast path the configs use (48 ... 384).  The
+    velocities agree to 1e-13; p, whose (0,0) Poisson solve amplifies
+    last-bit differences of its right-hand side, to 1e-12."""
     from lh_b200 import Desc, grids, perturbed_laminar
     d = Desc(Nx=N, Nz=N, ny=65, dt_mode=1, dt=1e-3)
     yu, yv = grids(d)
@@ -232,4 +235,4 @@ def test_fast_and_generic_fft_paths_agree(N, monkeypatch):
         e.synchronize()
         out.append(e.download())
     for f in FIELDS:
-        assert rel_l2(out[0][f], out[1][f]) <= 1e-13, f
+        assert rel_l2(out[0][f], out[1][f]) <= (1e-12 if f == "p" else 1e-13), f
