@@ -281,11 +281,12 @@ ClassTiles fast_tiles(const HostSetup &s, int cbz_max, int rb, int cbf_max)
     c.tx = fast_threads(s.Mx, 3 * rb);
     c.smx = (size_t)s.Mx * (1 + 3 * rb) * sizeof(double2);
     cbf_max = std::max(1, std::min(cbf_max, s.nxh));
-    while (cbf_max > 1 && !fits(2, s.Mz, 6 * cbf_max, 6 * cbf_max)) cbf_max--;
+    // z forward: one half of the six products (3 vectors per x mode) per CTA
+    while (cbf_max > 1 && !fits(2, s.Mz, 3 * cbf_max, 3 * cbf_max)) cbf_max--;
     nb = (s.nxh + cbf_max - 1) / cbf_max;
     c.cbf = (s.nxh + nb - 1) / nb;
-    c.tf = fast_threads(s.Mz, 6 * c.cbf);
-    c.smf = (size_t)s.Mz * (1 + 6 * c.cbf) * sizeof(double2);
+    c.tf = fast_threads(s.Mz, 3 * c.cbf);
+    c.smf = (size_t)s.Mz * (1 + 3 * c.cbf) * sizeof(double2);
     return c;
 }
 
@@ -298,8 +299,8 @@ ClassTiles class_tiles(const HostSetup &s, bool force_generic)
     if (c.fast && ov && sscanf(ov, "%d,%d,%d", &a, &b, &d) == 3 && a > 0 && b > 0 && d > 0) return fast_tiles(s, a, b, d);
     if (c.fast) {
         // measured on B200 at 128^2 and 32^2: 16 x modes per z-inverse CTA,
-        // 4 z rows per x CTA, up to 8 x modes per z-forward CTA
-        c = fast_tiles(s, 16, 4, 8);
+        // 4 z rows per x CTA, up to 5 x modes per z-forward CTA
+        c = fast_tiles(s, 16, 4, 5);
     } else {
         Tiles t = default_tiles(s.Mx, s.Mz, s.nxh, s.nyu);
         c.cbz = t.bc_zinv;
@@ -377,7 +378,8 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
                     }
                 for (int j = j0; j <= j1; j++) {
                     for (int b = 0; b < nbx; b++) L[1][cls_of[q]].push_back({q, j, j - j0, b});
-                    for (int b = 0; b < nbf; b++) L[2][cls_of[q]].push_back({q, j, j - j0, b});
+                    for (int b = 0; b < nbf; b++)
+                        for (int h = 0; h < 2; h++) L[2][cls_of[q]].push_back({q, j, j - j0, 2 * b + h});
                 }
             }
         } else {

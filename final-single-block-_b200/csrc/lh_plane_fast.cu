@@ -35,10 +35,10 @@
 #define LH_XPROD_B 3
 #endif
 #ifndef LH_ZFWD_T
-#define LH_ZFWD_T 512
+#define LH_ZFWD_T 256
 #endif
 #ifndef LH_ZFWD_B
-#define LH_ZFWD_B LH_FFT_MINB
+#define LH_ZFWD_B 3
 #endif
 #include "lh_kernels.cuh"
 
@@ -128,10 +128,12 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
     load_table(tw, insts[work[blockIdx.x].inst].twx, NX);  // depends on Mx only
     const int t = threadIdx.x, nv = 3 * rb, v = t % nv, r = t / nv;
     const int pr = v / rb, rr = v % rb;
+    constexpr int nxh = NX / 3 + 1;  // Nx/2 + 1 with Mx = 3 Nx / 2
+    const FastDiv by_rb(rb), by_nv(nv);
     {
         const Work w = work[blockIdx.x];
         const Inst &I = insts[w.inst];
-        const int Mz = I.Mz, nxh = I.nxh, j = w.j;
+        const int Mz = I.Mz, j = w.j;
         const int q0 = w.blk * rb;
         const size_t fs = (size_t)Mz * nxh;
         const double2 *u1j = sin_field(I, w.slot + 1, 0), *u3j = u1j + fs, *vj = u3j + fs;
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
         // (0) coalesced gather of the 6 fields x rb rows x (Nx/2+1) modes: in[f][rr][k]
         double2 *in = buf;
         for (int e = t; e < kNumProducts * rb * nxh; e += blockDim.x) {
-            const int k = e % nxh, fr = e / nxh, r2 = fr % rb, f = fr / rb;
+            const int fr = e / nxh, k = e - fr * nxh, f = by_rb.div(fr), r2 = by_rb.mod(fr, f);
             const int q = q0 + r2;
             double2 val = make_double2(0.0, 0.0);
             if (q < Mz) {
@@ -218,7 +220,7 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
         const bool track = want_max && I.dt_mode == 0 && j <= I.nyu - 1;
         double m1 = 0.0, m3 = 0.0;
         for (int e = t; e < NX * rb; e += blockDim.x) {
-            const int x = e / rb, r2 = e % rb;
+            const int x = by_rb.div(e), r2 = by_rb.mod(e, x);
             double2 *p = buf + x * nv;
             const double2 p0 = p[r2], p1 = p[rb + r2], p2 = p[2 * rb + r2];
             const double u1 = p0.x, u3 = p0.y, u2c = p1.x, u2 = p1.y, u1f = p2.x, u3f = p2.y;
@@ -287,11 +289,11 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
         // (6) split the packed real transforms, scale 1/Mx, keep modes i <= Nx/2
         const double dn1 = 1.0 / NX;
         for (int e = t; e < nxh * nv; e += blockDim.x) {
-            const int k = e / nv, vv = e % nv;
-            const int p2 = vv / rb, r2 = vv % rb, qq = q0 + r2;
+            const int k = by_nv.div(e), vv = by_nv.mod(e, k);
+            const int p2 = by_rb.div(vv), r2 = by_rb.mod(vv, p2), qq = q0 + r2;
             if (qq >= Mz) continue;
             const double2 zk = buf[k * nv + vv];
-            const double2 zm = buf[((NX - k) % NX) * nv + vv];
+            const double2 zm = buf[(k == 0 ? 0 : NX - k) * nv + vv];
             double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
             double2 B = make_double2(0.5 * (zk.y + zm.y), 0.5 * (zm.x - zk.x));
             if (k == 0) {
@@ -305,9 +307,11 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
 }
 
 // ---------------------------------------------------------------------------
-// z forward, masks and derivatives of one (plane, block of cb x modes):
+// z forward, masks and derivatives of one (plane, block of cb x modes, half):
 // phys_to_four_du's cft (FOU3D.f90:1654-1672), der_x/der_z (:420-523) and
-// planes_to_modes_UVP/NUVP -> NXZ1..3, UVF, WVF, VVC
+// planes_to_modes_UVP/NUVP.  The six products split into two independent
+// halves: {uu, uw, ww} -> Nu1 and Nu3 x/z parts; {vv, uv, wv} -> vv_c, uv_f,
+// wv_f and the Nu2 x/z part.
 template <int NZ>
 __global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
                                                          int count, int cb)
@@ -318,13 +322,16 @@ __global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_f(const Inst *__r
     double2 *tw = sm, *T = sm + NZ;
     if ((int)blockIdx.x >= count) return;
     load_table(tw, insts[work[blockIdx.x].inst].twz, NZ);  // depends on Mz only
-    const int t = threadIdx.x, nv = kNumProducts * cb, v = t % nv, r = t / nv;
+    const int t = threadIdx.x, nv = 3 * cb, v = t % nv, r = t / nv;
     const int f = v / cb, c = v % cb;
+    const FastDiv by_cb(cb);
     {
         const Work w = work[blockIdx.x];
         const Inst &I = insts[w.inst];
         const int nxh = I.nxh, nc = I.nc, j = w.j;
-        const int i0 = w.blk * cb, i = i0 + c;
+        const int h = w.blk & 1;
+        const int i0 = (w.blk >> 1) * cb, i = i0 + c;
+        const int g = h == 0 ? (f == 2 ? 3 : f) : (f == 0 ? 2 : f + 3);  // product of this vector
         const double2 *S = sprod_slot(I, w.slot);
         const bool ok = i < nxh;
         __syncthreads();  // table loaded / T free
@@ -332,7 +339,7 @@ __global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_f(const Inst *__r
             double2 a[N1];
 #pragma unroll
             for (int n1 = 0; n1 < N1; n1++)
-                a[n1] = ok ? S[((size_t)f * NZ + r + N2 * n1) * nxh + i] : make_double2(0.0, 0.0);
+                a[n1] = ok ? S[((size_t)g * NZ + r + N2 * n1) * nxh + i] : make_double2(0.0, 0.0);
             DFT<N1, -1, NZ>::run(a, tw);
 #pragma unroll
             for (int k1 = 0; k1 < N1; k1++) {
@@ -358,28 +365,31 @@ __global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_f(const Inst *__r
         }
         __syncthreads();
         for (int e = t; e < Nz * cb; e += blockDim.x) {
-            const int cc = e % cb, kr = e / cb, ii = i0 + cc;
+            const int kr = by_cb.div(e), cc = by_cb.mod(e, kr), ii = i0 + cc;
             if (ii >= nxh) continue;
             const int zp = kr < Nz / 2 ? kr : kr + NZ - Nz;
             const double2 *row = T + zp * nv + cc;
-            double2 pr[kNumProducts];
-#pragma unroll
-            for (int g = 0; g < kNumProducts; g++) pr[g] = row[g * cb];
-            const size_t o = (size_t)j * nc + kr * nxh + ii;
-            I.VVC[o] = pr[2];
-            I.UVF[o] = pr[4];
-            I.WVF[o] = pr[5];
-            double2 n1 = make_double2(0.0, 0.0), n2 = n1, n3 = n1;
-            if (kr != Nz / 2) {  // der_x/der_z zero the kz = -Nz/2 row (FOU3D.f90:444-447)
-                const double kx = I.kx[ii], kz = I.kz[kr];
-                n1 = make_double2(-(kx * pr[0].y) + -(kz * pr[1].y), kx * pr[0].x + kz * pr[1].x);
-                n3 = make_double2(-(kx * pr[1].y) + -(kz * pr[3].y), kx * pr[1].x + kz * pr[3].x);
-                n2 = make_double2(-(kx * pr[4].y) + -(kz * pr[5].y), kx * pr[4].x + kz * pr[5].x);
-            }
+            const double2 p0 = row[0], p1 = row[cb], p2 = row[2 * cb];
             const size_t on = (size_t)(j - 1) * nc + kr * nxh + ii;
-            I.NXZ1[on] = n1;
-            I.NXZ2[on] = n2;
-            I.NXZ3[on] = n3;
+            const bool keep = kr != Nz / 2;  // der_x/der_z zero the kz = -Nz/2 row (FOU3D.f90:444-447)
+            const double kx = I.kx[ii], kz = I.kz[kr];
+            if (h == 0) {  // p0 uu, p1 uw, p2 ww
+                double2 n1 = make_double2(0.0, 0.0), n3 = n1;
+                if (keep) {
+                    n1 = make_double2(-(kx * p0.y) + -(kz * p1.y), kx * p0.x + kz * p1.x);
+                    n3 = make_double2(-(kx * p1.y) + -(kz * p2.y), kx * p1.x + kz * p2.x);
+                }
+                I.NXZ1[on] = n1;
+                I.NXZ3[on] = n3;
+            } else {  // p0 vv, p1 uv, p2 wv
+                const size_t o = (size_t)j * nc + kr * nxh + ii;
+                I.VVC[o] = p0;
+                I.UVF[o] = p1;
+                I.WVF[o] = p2;
+                double2 n2 = make_double2(0.0, 0.0);
+                if (keep) n2 = make_double2(-(kx * p1.y) + -(kz * p2.y), kx * p1.x + kz * p2.x);
+                I.NXZ2[on] = n2;
+            }
         }
     }
 }
