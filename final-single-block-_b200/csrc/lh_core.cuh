@@ -79,6 +79,7 @@ struct Work {
     int j;      // plane (plane kernels) or column block (column kernel)
     int slot;   // staging slot of the plane
     int blk;    // sub-block
+    int aux;    // x stage: Sin slot of row j-1
 };
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }

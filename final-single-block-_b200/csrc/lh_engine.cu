@@ -14,9 +14,10 @@ namespace lh {
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Plane fields (Mz x nxh complex) of the staging buffer for `chunk` planes:
-// the fast path's Sin (chunk + 2 rows x 3 fields) and Sprod (chunk x 6);
-// the generic path uses the first 6 * chunk.
-size_t staging_units(int chunk) { return (size_t)(chunk + 2) * 3 + (size_t)chunk * kNumProducts; }
+// the fast path's Sin (chunk + 4 rows x 3 fields: two half-chunk rounds in
+// flight, each with a halo row on either side) and Sprod (chunk x 6); the
+// generic path uses the first 6 * chunk.
+size_t staging_units(int chunk) { return (size_t)(chunk + 4) * 3 + (size_t)chunk * kNumProducts; }
 
 // Bytes of plane staging one chunk round may use across all instances of a
 // plan, kept well inside the 126 MB L2 (LH_STAGING_MB overrides, for tuning).
@@ -39,7 +40,7 @@ Tiles default_tiles(int Mx, int Mz, int nxh, int nyu)
     // for the halo rows (staging_units), the generic path 6 per plane
     const size_t unit = (size_t)Mz * nxh * sizeof(double2);
     const size_t units = staging_budget() / unit;
-    t.chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nyu, units > 6 ? (units - 6) / 9 : 1));
+    t.chunk = (int)std::max<size_t>(2, std::min<size_t>((size_t)nyu + 1, units > 12 ? (units - 12) / 9 : 2));
     return t;
 }
 
@@ -349,8 +350,10 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
         const bool fast = tiles[cls_of[q]].fast;
         const size_t unit = (size_t)s.Mz * s.nxh * sizeof(double2);
         const size_t units = l2_budget / (unit * insts.size());
-        size_t c = fast ? (units > 6 ? (units - 6) / 9 : 1) : units / kNumProducts;
-        c = std::max<size_t>(1, std::min<size_t>(c, (size_t)insts[q]->inst.chunk));
+        // two rounds are in flight (even rounds on the main stream, odd ones
+        // on the side stream), each with half of the staging
+        size_t c = fast ? (units > 12 ? (units - 12) / 9 : 2) : units / kNumProducts;
+        c = std::max<size_t>(2, std::min<size_t>(c, (size_t)insts[q]->inst.chunk)) / 2;
         chunk_eff[q] = (int)c;
         rounds = std::max(rounds, (s.nyu + chunk_eff[q] - 1) / chunk_eff[q]);
     }
@@ -366,33 +369,36 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
         const int nbx = (s.Mz + ct.rbx - 1) / ct.rbx;
         const int nbf = (s.nxh + ct.cbf - 1) / ct.cbf;
         if (ct.fast) {
-            // round r: planes j0..j1; Sin slot p holds y row j0-1+p, u1/u3 on
-            // rows j0..j1+1 and u2 on rows j0-1..j1
+            // round r: planes j0..j1 in staging half r%2; Sin slot sb+p holds
+            // y row j0-1+p (u1/u3 on rows j0..j1+1, u2 on rows j0-1..j1),
+            // Sprod slot pb+j-j0 plane j
             for (int j0 = 1, r = 0; j0 <= s.nyu; j0 += chunk, r++) {
                 const int j1 = std::min(s.nyu, j0 + chunk - 1);
+                const int sb = (r % 2) * (chunk + 2), pb = (r % 2) * chunk;
                 auto &L = lists[r];
                 for (int jp = j0 - 1; jp <= j1 + 1; jp++)
                     for (int f = 0; f < 3; f++) {
                         if (f < 2 ? jp < j0 : jp > j1) continue;
-                        for (int b = 0; b < nbz; b++) L[0][cls_of[q]].push_back({q, jp, jp - j0 + 1, f * nbz + b});
+                        for (int b = 0; b < nbz; b++)
+                            L[0][cls_of[q]].push_back({q, jp, sb + jp - j0 + 1, f * nbz + b, 0});
                     }
                 for (int j = j0; j <= j1; j++) {
-                    for (int b = 0; b < nbx; b++) L[1][cls_of[q]].push_back({q, j, j - j0, b});
+                    for (int b = 0; b < nbx; b++) L[1][cls_of[q]].push_back({q, j, pb + j - j0, b, sb + j - j0});
                     for (int b = 0; b < nbf; b++)
-                        for (int h = 0; h < 2; h++) L[2][cls_of[q]].push_back({q, j, j - j0, 2 * b + h});
+                        for (int h = 0; h < 2; h++) L[2][cls_of[q]].push_back({q, j, pb + j - j0, 2 * b + h, 0});
                 }
             }
         } else {
             for (int j = 1; j <= s.nyu; j++) {
-                const int r = (j - 1) / chunk, slot = (j - 1) % chunk;
+                const int r = (j - 1) / chunk, slot = (r % 2) * chunk + (j - 1) % chunk;
                 auto &L = lists[r];
                 for (int f = 0; f < kNumProducts; f++)
-                    for (int b = 0; b < nbz; b++) L[0][cls_of[q]].push_back({q, j, slot, f * nbz + b});
-                for (int b = 0; b < nbx; b++) L[1][cls_of[q]].push_back({q, j, slot, b});
-                for (int b = 0; b < nbf; b++) L[2][cls_of[q]].push_back({q, j, slot, b});
+                    for (int b = 0; b < nbz; b++) L[0][cls_of[q]].push_back({q, j, slot, f * nbz + b, 0});
+                for (int b = 0; b < nbx; b++) L[1][cls_of[q]].push_back({q, j, slot, b, 0});
+                for (int b = 0; b < nbf; b++) L[2][cls_of[q]].push_back({q, j, slot, b, 0});
             }
         }
-        for (int b = 0; b < (s.nc + kColumnThreads - 1) / kColumnThreads; b++) p.column.push_back({q, b, 0, 0});
+        for (int b = 0; b < (s.nc + kColumnThreads - 1) / kColumnThreads; b++) p.column.push_back({q, b, 0, 0, 0});
     }
     std::vector<Work> all;
     p.rounds.assign(rounds, {});
@@ -417,7 +423,11 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
             }
     p.off_column = all.size();
     all.insert(all.end(), p.column.begin(), p.column.end());
-    cudaError_t e = cudaMalloc(&p.d_work, all.size() * sizeof(Work));
+    cudaError_t e = cudaStreamCreateWithFlags(&p.side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+    e = cudaMalloc(&p.d_work, all.size() * sizeof(Work));
     if (e != cudaSuccess) {
         p.d_work = nullptr;
         return e;
@@ -453,6 +463,11 @@ void plan_free(Plan &p)
 {
     if (p.d_work) cudaFree(p.d_work);
     p.d_work = nullptr;
+    if (p.ev_fork) cudaEventDestroy(p.ev_fork);
+    if (p.ev_join) cudaEventDestroy(p.ev_join);
+    if (p.side) cudaStreamDestroy(p.side);
+    p.ev_fork = p.ev_join = nullptr;
+    p.side = nullptr;
     p.rounds.clear();
 }
 
@@ -478,10 +493,20 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
 {
     const int want_max = (kRK == 1 && cfl_any) ? 1 : 0;
     cudaError_t e = cudaSuccess;
-    for (const auto &round : p.rounds)
-        for (const Group &g : round) {
+    // even rounds on st, odd rounds on the side stream (their staging halves
+    // are disjoint), forked after and joined before the work on st that the
+    // plane pass depends on / feeds; timed profiles keep one stream
+    const bool two = timer == nullptr && p.side != nullptr && p.rounds.size() > 1;
+    if (two) {
+        if ((e = cudaEventRecord(p.ev_fork, st)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(p.side, p.ev_fork, 0)) != cudaSuccess) return e;
+    }
+    for (size_t ri = 0; ri < p.rounds.size(); ri++)
+        for (const Group &g : p.rounds[ri]) {
             const Work *w = p.d_work + g.off;
             const unsigned n = (unsigned)g.count;
+            cudaStream_t st0 = st;
+            cudaStream_t st = (two && ri % 2 == 1) ? p.side : st0;
             time_begin(timer, st);
             if (g.fast) {
                 const int cnt = (int)g.count;
@@ -496,6 +521,10 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
             }
             if ((e = time_end(timer, g.stage, st)) != cudaSuccess) return e;
         }
+    if (two) {
+        if ((e = cudaEventRecord(p.ev_join, p.side)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(st, p.ev_join, 0)) != cudaSuccess) return e;
+    }
     if (kRK == 1) {
         time_begin(timer, st);
         k_dt<<<p.ninst, 256, 0, st>>>(d_insts, p.ninst);

@@ -72,6 +72,8 @@ struct Plan {
     size_t sm_col = 0;
     int ninst = 0;
     bool force_generic = false;
+    cudaStream_t side = nullptr;           // odd chunk rounds
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 // Optional per-launch timing (kernel classes 0 z inverse, 1 x products,

@@ -5,12 +5,12 @@
 // the Ngal sizes of the usual grids.  One CTA per work item; the twiddle
 // table is copied into shared memory per CTA.
 //
-// Staging (per instance, inside I.S):
-//   Sin  [cap+2][3][Mz][nxh]  z-inverse of u1, u3 and u2 on the y rows of
-//        the round's planes plus one halo row each side (slot p holds row
-//        j0-1+p); x stays spectral.
+// Staging (per instance, inside I.S; two chunk rounds in flight use
+// disjoint halves):
+//   Sin  [cap+4][3][Mz][nxh]  z-inverse of u1, u3 and u2 on the y rows of
+//        a round's planes plus one halo row each side; x stays spectral.
 //   Sprod[cap][6][Mz][nxh]    the six products after the forward x
-//        transform, one slot per plane of the round.
+//        transform, one slot per plane of a round.
 // The y interpolations of the reference (interp_u/interp_v, FOU3D.f90:
 // 373-418) are linear and commute with the z transform, so they are applied
 // to the z-transformed rows in the x stage: the z inverse runs on three
@@ -50,7 +50,7 @@ __device__ __forceinline__ double2 *sin_field(const Inst &I, int p, int f)
 }
 __device__ __forceinline__ double2 *sprod_slot(const Inst &I, int s)
 {
-    return I.S + ((size_t)(I.chunk + 2) * 3 + (size_t)s * kNumProducts) * I.Mz * I.nxh;
+    return I.S + ((size_t)(I.chunk + 4) * 3 + (size_t)s * kNumProducts) * I.Mz * I.nxh;
 }
 
 // ---------------------------------------------------------------------------
@@ -136,9 +136,9 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
         const int Mz = I.Mz, j = w.j;
         const int q0 = w.blk * rb;
         const size_t fs = (size_t)Mz * nxh;
-        const double2 *u1j = sin_field(I, w.slot + 1, 0), *u3j = u1j + fs, *vj = u3j + fs;
-        const double2 *vjm = sin_field(I, w.slot, 2);
-        const double2 *u1p = sin_field(I, w.slot + 2, 0), *u3p = u1p + fs;
+        const double2 *u1j = sin_field(I, w.aux + 1, 0), *u3j = u1j + fs, *vj = u3j + fs;
+        const double2 *vjm = sin_field(I, w.aux, 2);
+        const double2 *u1p = sin_field(I, w.aux + 2, 0), *u3p = u1p + fs;
         const double dnv = 1.0 / (I.yv[j] - I.yv[j - 1]), dnu = 1.0 / (I.yu[j + 1] - I.yu[j]);
         const double w0v = (I.yu[j] - I.yv[j - 1]) * dnv, w1v = (I.yv[j] - I.yu[j]) * dnv;
         const double w0u = (I.yv[j] - I.yu[j]) * dnu, w1u = (I.yu[j + 1] - I.yv[j]) * dnu;
