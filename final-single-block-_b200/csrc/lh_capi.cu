@@ -283,13 +283,13 @@ static int plane_transform(lh_ctx *c, double *planes, int nplanes, int sgn)
     const int nbz = (s.nxh + bc - 1) / bc, nbx = ((s.Mz + 1) / 2 + br - 1) / br;
     if (e == cudaSuccess) {
         if (sgn > 0) {
-            cudaFuncSetAttribute(k_plane_z_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
-            cudaFuncSetAttribute(k_plane_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
+            raise_smem_limit((const void *)k_plane_z_inv, smz);
+            raise_smem_limit((const void *)k_plane_x_inv, smx);
             k_plane_z_inv<<<nplanes * nbz, thr, smz, c->st>>>(c->d_inst, d, bc);
             k_plane_x_inv<<<nplanes * nbx, thr, smx, c->st>>>(c->d_inst, d, br);
         } else {
-            cudaFuncSetAttribute(k_plane_z_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
-            cudaFuncSetAttribute(k_plane_x_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
+            raise_smem_limit((const void *)k_plane_z_fwd, smz);
+            raise_smem_limit((const void *)k_plane_x_fwd, smx);
             k_plane_x_fwd<<<nplanes * nbx, thr, smx, c->st>>>(c->d_inst, d, br);
             k_plane_z_fwd<<<nplanes * nbz, thr, smz, c->st>>>(c->d_inst, d, bc);
             k_plane_zero_row<<<nplanes, 256, 0, c->st>>>(c->d_inst, d);

@@ -13,6 +13,17 @@ namespace lh {
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// A kernel's dynamic shared-memory limit is process-wide and captured graphs
+// of other plans may rely on it, so it is only ever raised.
+cudaError_t raise_smem_limit(const void *func, size_t bytes)
+{
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, func);
+    if (e != cudaSuccess) return e;
+    if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+    return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 // Plane fields (Mz x nxh complex) of the staging buffer for `chunk` planes:
 // the fast path's Sin (chunk + 4 rows x 3 fields: two half-chunk rounds in
 // flight, each with a halo row on either side) and Sprod (chunk x 6); the
@@ -299,9 +310,11 @@ ClassTiles class_tiles(const HostSetup &s, bool force_generic)
     int a = 0, b = 0, d = 0;
     if (c.fast && ov && sscanf(ov, "%d,%d,%d", &a, &b, &d) == 3 && a > 0 && b > 0 && d > 0) return fast_tiles(s, a, b, d);
     if (c.fast) {
-        // measured on B200 at 128^2 and 32^2: 16 x modes per z-inverse CTA,
-        // 4 z rows per x CTA, up to 5 x modes per z-forward CTA
-        c = fast_tiles(s, 16, 4, 5);
+        // measured on B200 at 128^2 (16 threads per vector): 16 x modes per
+        // z-inverse CTA, 4 z rows per x CTA, up to 5 x modes per z-forward
+        // CTA; sizes with fewer threads per vector take proportionally more
+        const int vz = std::max(1, fast_vector_threads(s.Mz)), vx = std::max(1, fast_vector_threads(s.Mx));
+        c = fast_tiles(s, 256 / vz, std::max(1, 64 / vx), std::max(1, 80 / vz));
     } else {
         Tiles t = default_tiles(s.Mx, s.Mz, s.nxh, s.nyu);
         c.cbz = t.bc_zinv;
@@ -447,16 +460,13 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
             gf = std::max(gf, tiles[c].smf);
         }
     }
-    if (gz && (e = cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gz)) != cudaSuccess)
-        return e;
-    if (gx && (e = cudaFuncSetAttribute(k_xprod, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gx)) != cudaSuccess)
-        return e;
-    if (gf && (e = cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gf)) != cudaSuccess)
-        return e;
+    if (gz && (e = raise_smem_limit((const void *)k_zinv, gz)) != cudaSuccess) return e;
+    if (gx && (e = raise_smem_limit((const void *)k_xprod, gx)) != cudaSuccess) return e;
+    if (gf && (e = raise_smem_limit((const void *)k_zfwd, gf)) != cudaSuccess) return e;
     int max_nyu = 1;
     for (const DevInstance *d : insts) max_nyu = std::max(max_nyu, d->hs.nyu);
     p.sm_col = column_smem_bytes(max_nyu);
-    return cudaFuncSetAttribute(k_column, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.sm_col);
+    return raise_smem_limit((const void *)k_column, p.sm_col);
 }
 
 void plan_free(Plan &p)

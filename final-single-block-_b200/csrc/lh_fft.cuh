@@ -165,13 +165,34 @@ struct DFT<4, SGN, NT> {
     static __device__ __forceinline__ void run(double2 *a, const double2 *) { dft4<SGN>(a[0], a[1], a[2], a[3]); }
 };
 
-// Two-pass split of a length-N transform.
+// Two-pass split N = N1 * N2 of a length-N transform: the pair with the
+// smallest max(N1, N2) (threads per vector are max(N1, N2), so a lopsided
+// split idles most of them in one pass), N1 in {16, 12, 9, 8, 6, 4, 3, 2},
+// N2 <= 24 and 3-smooth; ties keep the larger N1.
+constexpr bool smooth23(int n)
+{
+    while (n % 2 == 0) n /= 2;
+    while (n % 3 == 0) n /= 3;
+    return n == 1;
+}
+constexpr int plan2_n1(int N)
+{
+    const int cand[8] = {16, 12, 9, 8, 6, 4, 3, 2};
+    int best = 1, score = N;
+    for (int k = 0; k < 8; k++) {
+        const int c = cand[k];
+        if (N % c != 0 || N / c > 24 || !smooth23(N / c)) continue;
+        const int sc = c > N / c ? c : N / c;
+        if (sc < score) {
+            score = sc;
+            best = c;
+        }
+    }
+    return best;
+}
 template <int N>
 struct Plan2 {
-    static constexpr int N1 = (N % 16 == 0 && N / 16 <= 24) ? 16
-                              : (N % 8 == 0 && N / 8 <= 24) ? 8
-                              : (N % 4 == 0 && N / 4 <= 24) ? 4
-                              : (N % 2 == 0) ? 2 : 1;
+    static constexpr int N1 = plan2_n1(N);
     static constexpr int N2 = N / N1;
 };
 

@@ -27,10 +27,14 @@ __global__ void k_lusolu(const Inst *__restrict__ insts, int grid, int kRK, doub
 __global__ void k_lusolp(const Inst *__restrict__ insts, double2 *x);
 __global__ void k_divmax(const Inst *__restrict__ insts, double *out);
 
+// raise (never lower) a kernel's dynamic shared-memory limit (lh_engine.cu)
+cudaError_t raise_smem_limit(const void *func, size_t bytes);
+
 // compile-time-sized fast path (lh_plane_fast.cu)
 bool fast_size(int n);
 int fast_threads(int n, int vectors);
 int fast_max_threads(int stage);  // launch-bounds block size of a fast stage
+int fast_vector_threads(int n);   // threads per vector of a fast length
 cudaError_t fast_set_attributes(int Mz, int Mx, size_t smz, size_t smx, size_t smf);
 void fast_launch_zinv(int Mz, unsigned grid, int threads, size_t smem, cudaStream_t st, const Inst *insts,
                       const Work *work, int count, int cb);

@@ -410,6 +410,20 @@ bool fast_size(int n)
     }
 }
 
+// Threads one vector of length n uses: max(N1, N2) of its two-pass split.
+int fast_vector_threads(int n)
+{
+    switch (n) {
+#define LH_CASE(N) \
+    case N:        \
+        return Plan2<N>::N1 > Plan2<N>::N2 ? Plan2<N>::N1 : Plan2<N>::N2;
+        LH_FAST_SIZES(LH_CASE)
+#undef LH_CASE
+    default:
+        return 0;
+    }
+}
+
 int fast_threads(int n, int vectors)
 {
     int n1 = 1, n2 = 1;
@@ -432,11 +446,10 @@ cudaError_t fast_set_attributes(int Mz, int Mx, size_t smz, size_t smx, size_t s
 {
     cudaError_t e = cudaSuccess;
     switch (Mz) {
-#define LH_CASE(N)                                                   \
-    case N:                                                          \
-        e = cudaFuncSetAttribute(k_zinv_f<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz); \
-        if (e == cudaSuccess)                                        \
-            e = cudaFuncSetAttribute(k_zfwd_f<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf); \
+#define LH_CASE(N)                                        \
+    case N:                                               \
+        e = raise_smem_limit((const void *)k_zinv_f<N>, smz); \
+        if (e == cudaSuccess) e = raise_smem_limit((const void *)k_zfwd_f<N>, smf); \
         break;
         LH_FAST_SIZES(LH_CASE)
 #undef LH_CASE
@@ -445,9 +458,9 @@ cudaError_t fast_set_attributes(int Mz, int Mx, size_t smz, size_t smx, size_t s
     }
     if (e != cudaSuccess) return e;
     switch (Mx) {
-#define LH_CASE(N)                                                   \
-    case N:                                                          \
-        e = cudaFuncSetAttribute(k_xprod_f<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx); \
+#define LH_CASE(N)                                         \
+    case N:                                                \
+        e = raise_smem_limit((const void *)k_xprod_f<N>, smx); \
         break;
         LH_FAST_SIZES(LH_CASE)
 #undef LH_CASE
