@@ -32,7 +32,27 @@ struct lh_batch {
     bool dirty = true;
     bool any_cfl = false;
     std::string err;
+    // device blocks of retired instances, reused by later admissions so a
+    // request stream does not pay cudaMalloc/cudaFree (a device-wide
+    // synchronisation) per request
+    struct Block {
+        void *ptr;
+        size_t bytes;
+    };
+    std::vector<Block> pool;
+    size_t pooled = 0;
 };
+
+static constexpr size_t kPoolBlocks = 16;
+
+static void pool_release(lh_batch *b, size_t keep_bytes)
+{
+    while (!b->pool.empty() && b->pooled > keep_bytes) {
+        cudaFree(b->pool.front().ptr);
+        b->pooled -= b->pool.front().bytes;
+        b->pool.erase(b->pool.begin());
+    }
+}
 
 static int bfail(lh_batch *b, int code, const std::string &m)
 {
@@ -86,6 +106,7 @@ extern "C" int lh_batch_destroy(lh_batch *b)
     if (b->d_insts) cudaFree(b->d_insts);
     for (auto &s : b->slots)
         if (s) instance_free(*s);
+    pool_release(b, 0);
     if (b->st) cudaStreamDestroy(b->st);
     delete b;
     return LH_OK;
@@ -117,7 +138,26 @@ extern "C" int lh_batch_add(lh_batch *b, const lh_grid_desc *desc, const double 
         return bfail(b, LH_ENOMEM, "HBM budget exhausted");
     // instances are admitted between steps; wait for in-flight work first
     BCK(cudaStreamSynchronize(b->st), "synchronize");
-    cudaError_t e = instance_alloc(*d, t.chunk, b->st);
+    // smallest pooled block that fits; else make room under the budget and allocate
+    int pick = -1;
+    for (size_t k = 0; k < b->pool.size(); k++)
+        if (b->pool[k].bytes >= need && (pick < 0 || b->pool[k].bytes < b->pool[pick].bytes)) pick = (int)k;
+    void *reuse = nullptr;
+    size_t reuse_bytes = 0;
+    if (pick >= 0) {
+        reuse = b->pool[pick].ptr;
+        reuse_bytes = b->pool[pick].bytes;
+        b->pooled -= reuse_bytes;
+        b->pool.erase(b->pool.begin() + pick);
+    } else if (b->budget) {
+        pool_release(b, b->budget > b->used + need ? b->budget - b->used - need : 0);
+    }
+    cudaError_t e = instance_alloc(*d, t.chunk, b->st, reuse, reuse_bytes);
+    if (e == cudaErrorMemoryAllocation && !reuse && !b->pool.empty()) {
+        cudaGetLastError();
+        pool_release(b, 0);
+        e = instance_alloc(*d, t.chunk, b->st);
+    }
     if (e == cudaSuccess) e = instance_upload(*d, u1, u2, u3, p, b->st);
     if (e != cudaSuccess) {
         instance_free(*d);
@@ -145,7 +185,15 @@ extern "C" int lh_batch_remove(lh_batch *b, int slot)
     if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot]) return bfail(b, LH_EINVAL, "bad slot");
     BCK(cudaStreamSynchronize(b->st), "synchronize");
     b->used -= b->slots[slot]->bytes;
-    instance_free(*b->slots[slot]);
+    DevInstance &d = *b->slots[slot];
+    b->pool.push_back({d.block, d.alloc_bytes});
+    b->pooled += d.alloc_bytes;
+    d.block = nullptr;
+    if (b->pool.size() > kPoolBlocks) {
+        cudaFree(b->pool.front().ptr);
+        b->pooled -= b->pool.front().bytes;
+        b->pool.erase(b->pool.begin());
+    }
     b->slots[slot].reset();
     b->dirty = true;
     return LH_OK;

@@ -127,7 +127,7 @@ size_t instance_bytes(const HostSetup &hs, int chunk)
     return c.off;
 }
 
-cudaError_t instance_alloc(DevInstance &d, int chunk, cudaStream_t st)
+cudaError_t instance_alloc(DevInstance &d, int chunk, cudaStream_t st, void *reuse, size_t reuse_bytes)
 {
     const HostSetup &s = d.hs;
     Carver c;
@@ -135,10 +135,17 @@ cudaError_t instance_alloc(DevInstance &d, int chunk, cudaStream_t st)
     memset(&I, 0, sizeof(I));
     carve(s, chunk, c, I, &d.stage, &d.stage_elems);
     d.bytes = c.off;
-    cudaError_t e = cudaMalloc(&d.block, d.bytes);
-    if (e != cudaSuccess) {
-        d.block = nullptr;
-        return e;
+    cudaError_t e = cudaSuccess;
+    if (reuse && reuse_bytes >= d.bytes) {
+        d.block = reuse;
+        d.alloc_bytes = reuse_bytes;
+    } else {
+        e = cudaMalloc(&d.block, d.bytes);
+        if (e != cudaSuccess) {
+            d.block = nullptr;
+            return e;
+        }
+        d.alloc_bytes = d.bytes;
     }
     c = Carver();
     c.base = (char *)d.block;
@@ -331,7 +338,9 @@ ClassTiles class_tiles(const HostSetup &s, bool force_generic)
 
 cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, bool force_generic)
 {
-    plan_free(p);
+    // the work buffer, side stream and events survive a rebuild
+    p.rounds.clear();
+    p.column.clear();
     p.force_generic = force_generic;
     p.ninst = (int)insts.size();
     // size classes in order of first appearance
@@ -364,9 +373,13 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
         const size_t unit = (size_t)s.Mz * s.nxh * sizeof(double2);
         const size_t units = l2_budget / (unit * insts.size());
         // two rounds are in flight (even rounds on the main stream, odd ones
-        // on the side stream), each with half of the staging
+        // on the side stream), each with half of the staging.  The L2 share
+        // shrinks with the number of instances; below nyu/8 planes per round
+        // the launch count costs more than staging spilling to HBM, so that
+        // is the floor (within the allocated capacity).
         size_t c = fast ? (units > 12 ? (units - 12) / 9 : 2) : units / kNumProducts;
-        c = std::max<size_t>(2, std::min<size_t>(c, (size_t)insts[q]->inst.chunk)) / 2;
+        c = std::max<size_t>(c / 2, (size_t)(s.nyu + 7) / 8);
+        c = std::max<size_t>(1, std::min<size_t>(c, (size_t)insts[q]->inst.chunk / 2));
         chunk_eff[q] = (int)c;
         rounds = std::max(rounds, (s.nyu + chunk_eff[q] - 1) / chunk_eff[q]);
     }
@@ -436,14 +449,21 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
             }
     p.off_column = all.size();
     all.insert(all.end(), p.column.begin(), p.column.end());
-    cudaError_t e = cudaStreamCreateWithFlags(&p.side, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.ev_fork, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.ev_join, cudaEventDisableTiming);
+    cudaError_t e = cudaSuccess;
+    if (!p.side) e = cudaStreamCreateWithFlags(&p.side, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !p.ev_fork) e = cudaEventCreateWithFlags(&p.ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess && !p.ev_join) e = cudaEventCreateWithFlags(&p.ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) return e;
-    e = cudaMalloc(&p.d_work, all.size() * sizeof(Work));
-    if (e != cudaSuccess) {
+    if (all.size() > p.work_cap) {
+        if (p.d_work) cudaFree(p.d_work);
         p.d_work = nullptr;
-        return e;
+        p.work_cap = 0;
+        e = cudaMalloc(&p.d_work, all.size() * sizeof(Work));
+        if (e != cudaSuccess) {
+            p.d_work = nullptr;
+            return e;
+        }
+        p.work_cap = all.size();
     }
     e = cudaMemcpy(p.d_work, all.data(), all.size() * sizeof(Work), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return e;
@@ -473,6 +493,7 @@ void plan_free(Plan &p)
 {
     if (p.d_work) cudaFree(p.d_work);
     p.d_work = nullptr;
+    p.work_cap = 0;
     if (p.ev_fork) cudaEventDestroy(p.ev_fork);
     if (p.ev_join) cudaEventDestroy(p.ev_join);
     if (p.side) cudaStreamDestroy(p.side);

@@ -32,7 +32,8 @@ struct DevInstance {
     lh_grid_desc desc{};
     Inst inst{};           // host copy with device pointers
     void *block = nullptr; // the allocation
-    size_t bytes = 0;
+    size_t bytes = 0;      // bytes the instance uses
+    size_t alloc_bytes = 0;  // size of the allocation (>= bytes when a pooled block is reused)
     double2 *stage = nullptr;  // layout-transform staging (one field)
     size_t stage_elems = 0;
 };
@@ -42,7 +43,9 @@ size_t staging_units(int chunk);
 // Bytes one instance needs for a staging chunk of `chunk` planes.
 size_t instance_bytes(const HostSetup &hs, int chunk);
 // Allocate and fill the device arrays of an instance (synchronous).
-cudaError_t instance_alloc(DevInstance &d, int chunk, cudaStream_t st);
+// With `reuse` (a device block of reuse_bytes from an earlier instance) the
+// instance is carved from it when it is large enough, instead of cudaMalloc.
+cudaError_t instance_alloc(DevInstance &d, int chunk, cudaStream_t st, void *reuse = nullptr, size_t reuse_bytes = 0);
 void instance_free(DevInstance &d);
 // Upload / download the four state fields in the reference column layout.
 cudaError_t instance_upload(DevInstance &d, const double *u1, const double *u2, const double *u3, const double *p,
@@ -68,6 +71,7 @@ struct Plan {
     std::vector<std::vector<Group>> rounds;  // launch order within a round
     std::vector<Work> column;
     Work *d_work = nullptr;  // all tables back to back
+    size_t work_cap = 0;     // Work entries d_work holds (reused across rebuilds)
     size_t off_column = 0;
     size_t sm_col = 0;
     int ninst = 0;

@@ -4,7 +4,9 @@
 // a Fortran real**integer with a run-time exponent is evaluated.
 #include "lh_setup.h"
 
+#include <algorithm>
 #include <cmath>
+#include <thread>
 #include <sstream>
 
 namespace lh {
@@ -202,35 +204,60 @@ std::string build_setup(const lh_grid_desc &d, HostSetup &s)
     for (int jj = ns + 1; jj <= ne; jj++) s.DG1[jj] = V(Db, jj - 1) * V(Gb, jj - 1);
     s.DG2.assign((size_t)len * nc, 0.0);
     s.DG3.assign((size_t)len * nc, 0.0);
-    std::vector<double> a1(len + 1), a2(len + 1), a3(len + 1);
+    // Row by row over all columns (the recurrence runs along y, columns are
+    // independent), so the plane-major DG rows are written contiguously; per
+    // element the operations and their order are those of LU_decP.
+    std::vector<double> k2x_c(nc), k2z_c(nc), a2p(nc), a3p(nc);
     for (int col = 0; col < nc; col++) {
-        const int i = col % s.nxh, kr = col / s.nxh;
-        const double k2x = s.k2x[i], k2z = s.k2z[kr];
-        a2[ns] = (V(Dt, ns) * V(Gb, ns)) + k2x + k2z;
-        a3[ns] = (V(Dt, ns) * V(Gt, ns + 1));
-        a1[ns] = 0.0;
-        a2[ne] = (V(Db, ne - 1) * V(Gt, ne)) + k2x + k2z;
-        a1[ne] = (V(Db, ne - 1) * V(Gb, ne - 1));
-        a3[ne] = 0.0;
-        for (int jj = ns + 1; jj <= ne - 1; jj++) {
-            a2[jj] = (V(Db, jj - 1) * V(Gt, jj)) + (V(Dt, jj) * V(Gb, jj)) + k2x + k2z;
-            a1[jj] = (V(Db, jj - 1) * V(Gb, jj - 1));
-            a3[jj] = (V(Dt, jj) * V(Gt, jj + 1));
+        k2x_c[col] = s.k2x[col % s.nxh];
+        k2z_c[col] = s.k2z[col / s.nxh];
+    }
+    auto factor_columns = [&](int c0, int c1) {
+        {
+            const double dg = V(Dt, ns) * V(Gb, ns), a3r = V(Dt, ns) * V(Gt, ns + 1);
+            for (int col = c0; col < c1; col++) {
+                double a2 = (dg + k2x_c[col]) + k2z_c[col], a3 = a3r;
+                if (col == 0) {  // gauge row of the (0,0) mode (tridLU_3D.f90:276-280)
+                    a2 = 1.0 / ((yu[1 + 1] - yu[1]) * (yu[1 + 1] - yu[1]));
+                    a3 = 0.0;
+                }
+                a2p[col] = 1.0 / a2;
+                a3p[col] = a3;
+            }
         }
-        if (col == 0) {  // gauge row of the (0,0) mode (tridLU_3D.f90:276-280)
-            a1[ns] = 0.0;
-            a2[ns] = 1.0 / ((yu[1 + 1] - yu[1]) * (yu[1 + 1] - yu[1]));
-            a3[ns] = 0.0;
-        }
-        a2[ns] = 1.0 / a2[ns];
         for (int jj = ns + 1; jj <= ne; jj++) {
-            a3[jj - 1] = a3[jj - 1] * a2[jj - 1];
-            a2[jj] = 1.0 / (a2[jj] - a1[jj] * a3[jj - 1]);
+            const double a1 = V(Db, jj - 1) * V(Gb, jj - 1);
+            const double b1 = V(Db, jj - 1) * V(Gt, jj);
+            const double b2 = jj < ne ? V(Dt, jj) * V(Gb, jj) : 0.0;
+            const double a3r = jj < ne ? V(Dt, jj) * V(Gt, jj + 1) : 0.0;
+            double *dg2p = &s.DG2[(size_t)(jj - 2) * nc], *dg3p = &s.DG3[(size_t)(jj - 2) * nc];
+            for (int col = c0; col < c1; col++) {
+                const double a3s = a3p[col] * a2p[col];  // a3(jj-1) scaled by its pivot
+                dg2p[col] = a2p[col];
+                dg3p[col] = a3s;
+                const double raw = jj < ne ? ((b1 + b2) + k2x_c[col]) + k2z_c[col] : (b1 + k2x_c[col]) + k2z_c[col];
+                a2p[col] = 1.0 / (raw - a1 * a3s);
+                a3p[col] = a3r;
+            }
         }
-        for (int jj = ns; jj <= ne; jj++) {
-            s.DG2[(size_t)(jj - 1) * nc + col] = a2[jj];
-            s.DG3[(size_t)(jj - 1) * nc + col] = a3[jj];
+        for (int col = c0; col < c1; col++) {
+            s.DG2[(size_t)(ne - 1) * nc + col] = a2p[col];
+            s.DG3[(size_t)(ne - 1) * nc + col] = 0.0;
         }
+    };
+    // large instances: column ranges on several host threads
+    const size_t work = (size_t)nc * len;
+    int nth = work > (1u << 20) ? (int)std::min<unsigned>(8u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    if (nth > 1) {
+        std::vector<std::thread> pool;
+        const int per = (nc + nth - 1) / nth;
+        for (int t = 0; t < nth; t++) {
+            const int c0 = t * per, c1 = std::min(nc, c0 + per);
+            if (c0 < c1) pool.emplace_back(factor_columns, c0, c1);
+        }
+        for (auto &th : pool) th.join();
+    } else {
+        factor_columns(0, nc);
     }
 
     // ---- twiddles: z with the rotation recurrence of cffti1

@@ -368,12 +368,24 @@ class Batch:
         return {"t": t.value, "dt": dt.value, "iter": it.value}
 
 
+_grid_cache: dict = {}
+
+
 def host_grid(desc: Desc, which: int) -> np.ndarray:
-    """Set-up arrays of a description computed on the host (no GPU needed)."""
-    L = lib()
-    n = L.lh_host_grid(ctypes.byref(desc.c()), which, None, 0)
-    if n < 0:
-        raise LHError(n, f"set-up rejected for {desc}")
-    out = np.zeros(n)
-    L.lh_host_grid(ctypes.byref(desc.c()), which, _dp(out), n)
-    return out
+    """Set-up arrays of a description computed on the host (no GPU needed);
+    memoised on the fields the y grid depends on (sizes, box and grid
+    stretching), a copy is returned."""
+    key = (desc.Nx, desc.Nz, desc.ny, desc.alp, desc.bet, desc.grid_type, desc.dyq, desc.ppp, desc.gamma,
+           desc.Re if which == 4 else None, which)
+    hit = _grid_cache.get(key)
+    if hit is None:
+        L = lib()
+        n = L.lh_host_grid(ctypes.byref(desc.c()), which, None, 0)
+        if n < 0:
+            raise LHError(n, f"set-up rejected for {desc}")
+        hit = np.zeros(n)
+        L.lh_host_grid(ctypes.byref(desc.c()), which, _dp(hit), n)
+        if len(_grid_cache) > 256:
+            _grid_cache.clear()
+        _grid_cache[key] = hit
+    return hit.copy()

@@ -88,13 +88,16 @@ def perturbed_laminar(desc: Desc, seed: int, yu: np.ndarray, yv: np.ndarray, amp
     env = amp * np.exp(-(kx ** 2 + kzv ** 2) / 16.0)
     out = []
     for f, y in ((0, yu), (1, yv), (2, yu)):
-        J = np.arange(y.size) if white_in_y else np.zeros(y.size, np.int64)
-        I2, J2 = np.meshgrid(i, J, indexing="ij")
-        K2, _ = np.meshgrid(kz, J, indexing="ij")
-        gr = _gauss(seed, f, I2, K2, J2, 0)
-        gi = _gauss(seed, f, I2, K2, J2, 1)
+        if white_in_y:
+            J = np.arange(y.size)
+            I2, J2 = np.meshgrid(i, J, indexing="ij")
+            K2, _ = np.meshgrid(kz, J, indexing="ij")
+            g = _gauss(seed, f, I2, K2, J2, 0) + 1j * _gauss(seed, f, I2, K2, J2, 1)
+        else:  # one coefficient per column (counter j = 0), shared by every row
+            j0 = np.zeros(nc, np.int64)
+            g = (_gauss(seed, f, i, kz, j0, 0) + 1j * _gauss(seed, f, i, kz, j0, 1))[:, None]
         prof = (1.0 - np.clip(y, -1.0, 1.0) ** 2) ** 2
-        a = env[:, None] * prof[None, :] * (gr + 1j * gi)
+        a = env[:, None] * prof[None, :] * g
         a[0, :] = 0.0  # mode (0,0) carries the mean profile only
         # Hermitian kx = 0 column: u(0,-kz) = conj(u(0,kz)); kz = -Nz/2 real
         nxh = desc.Nx // 2 + 1
