@@ -240,6 +240,23 @@ def batched_and_served(args):
     return batched, served
 
 
+def max_over_ranks(vals, world, device):
+    """Element-wise maximum of a list of floats over all ranks (all_reduce MAX);
+    the identity at world size 1."""
+    import torch
+    t = torch.tensor(vals, dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as tdist
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def job_rate(world, units_per_rank, seconds):
+    """Whole-job throughput: the units all ranks processed over the slowest
+    rank's time (each rank runs its own instance, weak scaling)."""
+    return world * units_per_rank / seconds
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from lh_b200 import Engine, grids, perturbed_laminar
@@ -268,11 +285,8 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     e.synchronize()  # error word: non-finite state fails the run
-    tmax = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        tdist.all_reduce(tmax, op=tdist.ReduceOp.MAX)
-    ms_max = float(tmax.item())
-    value = world * pts_sub * K / (ms_max * 1e-3)
+    (ms_max,) = max_over_ranks([ms], world, "cuda")
+    value = job_rate(world, pts_sub * K, ms_max * 1e-3)
     launches_per_step = None
 
     # per-kernel breakdown with CUDA events on the engine's stream
@@ -310,14 +324,17 @@ def run_ours(args, rank, world, local_rank):
     e.step_host(addrs, 1)  # warm
     if dist:
         tdist.barrier()
-    t0 = time.perf_counter()
+    # device time on the engine's stream around the host-buffer calls: each
+    # call uploads, steps and downloads on that stream before it returns
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev2.record(st)
     for _ in range(Ke):
         e.step_host(addrs, 1)
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if dist:
-        tdist.all_reduce(te, op=tdist.ReduceOp.MAX)
-    e2e_val = world * pts_sub * Ke / float(te.item())
+    ev3.record(st)
+    ev3.synchronize()
+    (e2e_ms,) = max_over_ranks([ev2.elapsed_time(ev3)], world, "cuda")
+    e2e_val = job_rate(world, pts_sub * Ke, e2e_ms * 1e-3)
 
     batched = served = None
     if rank == 0 and world == 1 and not args.no_serve:
