@@ -19,6 +19,12 @@ namespace lh {
 
 constexpr int kMaxRad = 12;
 constexpr int kNumProducts = 6;
+// Chunk rounds of the plane pipeline in flight at once, on as many streams,
+// each with its own share of the staging.
+#ifndef LH_ROUND_STREAMS
+#define LH_ROUND_STREAMS 2
+#endif
+constexpr int kRoundStreams = LH_ROUND_STREAMS;
 
 // Radix-3 constant exactly as the reference's FFTPACK carries it
 // (cft_buff.f:333, rft_buff.f:364): 15 significant digits.

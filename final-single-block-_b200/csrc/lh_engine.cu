@@ -25,10 +25,10 @@ cudaError_t raise_smem_limit(const void *func, size_t bytes)
 }
 
 // Plane fields (Mz x nxh complex) of the staging buffer for `chunk` planes:
-// the fast path's Sin (chunk + 4 rows x 3 fields: two half-chunk rounds in
-// flight, each with a halo row on either side) and Sprod (chunk x 6); the
-// generic path uses the first 6 * chunk.
-size_t staging_units(int chunk) { return (size_t)(chunk + 4) * 3 + (size_t)chunk * kNumProducts; }
+// the fast path's Sin (chunk + 2 kRoundStreams rows x 3 fields: the rounds in
+// flight each hold a share of the chunk plus a halo row on either side) and
+// Sprod (chunk x 6); the generic path uses the first 6 * chunk.
+size_t staging_units(int chunk) { return (size_t)(chunk + 2 * kRoundStreams) * 3 + (size_t)chunk * kNumProducts; }
 
 // Bytes of plane staging one chunk round may use across all instances of a
 // plan, kept well inside the 126 MB L2 (LH_STAGING_MB overrides, for tuning).
@@ -51,7 +51,9 @@ Tiles default_tiles(int Mx, int Mz, int nxh, int nyu)
     // for the halo rows (staging_units), the generic path 6 per plane
     const size_t unit = (size_t)Mz * nxh * sizeof(double2);
     const size_t units = staging_budget() / unit;
-    t.chunk = (int)std::max<size_t>(2, std::min<size_t>((size_t)nyu + 1, units > 12 ? (units - 12) / 9 : 2));
+    const size_t fixed = 6 * kRoundStreams;
+    t.chunk = (int)std::max<size_t>(kRoundStreams, std::min<size_t>((size_t)nyu + kRoundStreams - 1,
+                                                                  units > fixed ? (units - fixed) / 9 : kRoundStreams));
     return t;
 }
 
@@ -372,14 +374,15 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
         const bool fast = tiles[cls_of[q]].fast;
         const size_t unit = (size_t)s.Mz * s.nxh * sizeof(double2);
         const size_t units = l2_budget / (unit * insts.size());
-        // two rounds are in flight (even rounds on the main stream, odd ones
-        // on the side stream), each with half of the staging.  The L2 share
+        // kRoundStreams rounds are in flight (round r on stream r %
+        // kRoundStreams), each with its share of the staging.  The L2 share
         // shrinks with the number of instances; below nyu/8 planes per round
         // the launch count costs more than staging spilling to HBM, so that
         // is the floor (within the allocated capacity).
-        size_t c = fast ? (units > 12 ? (units - 12) / 9 : 2) : units / kNumProducts;
-        c = std::max<size_t>(c / 2, (size_t)(s.nyu + 7) / 8);
-        c = std::max<size_t>(1, std::min<size_t>(c, (size_t)insts[q]->inst.chunk / 2));
+        const size_t fixed = 6 * kRoundStreams;
+        size_t c = fast ? (units > fixed ? (units - fixed) / 9 : kRoundStreams) : units / kNumProducts;
+        c = std::max<size_t>(c / kRoundStreams, (size_t)(s.nyu + 7) / 8);
+        c = std::max<size_t>(1, std::min<size_t>(c, (size_t)insts[q]->inst.chunk / kRoundStreams));
         chunk_eff[q] = (int)c;
         rounds = std::max(rounds, (s.nyu + chunk_eff[q] - 1) / chunk_eff[q]);
     }
@@ -400,7 +403,7 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
             // Sprod slot pb+j-j0 plane j
             for (int j0 = 1, r = 0; j0 <= s.nyu; j0 += chunk, r++) {
                 const int j1 = std::min(s.nyu, j0 + chunk - 1);
-                const int sb = (r % 2) * (chunk + 2), pb = (r % 2) * chunk;
+                const int sb = (r % kRoundStreams) * (chunk + 2), pb = (r % kRoundStreams) * chunk;
                 auto &L = lists[r];
                 for (int jp = j0 - 1; jp <= j1 + 1; jp++)
                     for (int f = 0; f < 3; f++) {
@@ -416,7 +419,7 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
             }
         } else {
             for (int j = 1; j <= s.nyu; j++) {
-                const int r = (j - 1) / chunk, slot = (r % 2) * chunk + (j - 1) % chunk;
+                const int r = (j - 1) / chunk, slot = (r % kRoundStreams) * chunk + (j - 1) % chunk;
                 auto &L = lists[r];
                 for (int f = 0; f < kNumProducts; f++)
                     for (int b = 0; b < nbz; b++) L[0][cls_of[q]].push_back({q, j, slot, f * nbz + b, 0});
@@ -450,9 +453,11 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
     p.off_column = all.size();
     all.insert(all.end(), p.column.begin(), p.column.end());
     cudaError_t e = cudaSuccess;
-    if (!p.side) e = cudaStreamCreateWithFlags(&p.side, cudaStreamNonBlocking);
-    if (e == cudaSuccess && !p.ev_fork) e = cudaEventCreateWithFlags(&p.ev_fork, cudaEventDisableTiming);
-    if (e == cudaSuccess && !p.ev_join) e = cudaEventCreateWithFlags(&p.ev_join, cudaEventDisableTiming);
+    if (!p.ev_fork) e = cudaEventCreateWithFlags(&p.ev_fork, cudaEventDisableTiming);
+    for (int k = 0; k < kRoundStreams - 1 && e == cudaSuccess; k++) {
+        if (!p.side[k]) e = cudaStreamCreateWithFlags(&p.side[k], cudaStreamNonBlocking);
+        if (e == cudaSuccess && !p.ev_join[k]) e = cudaEventCreateWithFlags(&p.ev_join[k], cudaEventDisableTiming);
+    }
     if (e != cudaSuccess) return e;
     if (all.size() > p.work_cap) {
         if (p.d_work) cudaFree(p.d_work);
@@ -495,10 +500,13 @@ void plan_free(Plan &p)
     p.d_work = nullptr;
     p.work_cap = 0;
     if (p.ev_fork) cudaEventDestroy(p.ev_fork);
-    if (p.ev_join) cudaEventDestroy(p.ev_join);
-    if (p.side) cudaStreamDestroy(p.side);
-    p.ev_fork = p.ev_join = nullptr;
-    p.side = nullptr;
+    p.ev_fork = nullptr;
+    for (int k = 0; k < kRoundStreams - 1; k++) {
+        if (p.ev_join[k]) cudaEventDestroy(p.ev_join[k]);
+        if (p.side[k]) cudaStreamDestroy(p.side[k]);
+        p.ev_join[k] = nullptr;
+        p.side[k] = nullptr;
+    }
     p.rounds.clear();
 }
 
@@ -524,20 +532,24 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
 {
     const int want_max = (kRK == 1 && cfl_any) ? 1 : 0;
     cudaError_t e = cudaSuccess;
-    // even rounds on st, odd rounds on the side stream (their staging halves
-    // are disjoint), forked after and joined before the work on st that the
-    // plane pass depends on / feeds; timed profiles keep one stream
-    const bool two = timer == nullptr && p.side != nullptr && p.rounds.size() > 1;
-    if (two) {
+    // round r on stream r % kRoundStreams (0 = st; their staging shares are
+    // disjoint), forked from st after the work the plane pass depends on and
+    // joined back before the work that consumes it; timed profiles keep one
+    // stream
+    const int nstreams = (timer == nullptr && p.side[0] != nullptr)
+                             ? (int)std::min<size_t>(kRoundStreams, p.rounds.size()) : 1;
+    if (nstreams > 1) {
         if ((e = cudaEventRecord(p.ev_fork, st)) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(p.side, p.ev_fork, 0)) != cudaSuccess) return e;
+        for (int k = 0; k < nstreams - 1; k++)
+            if ((e = cudaStreamWaitEvent(p.side[k], p.ev_fork, 0)) != cudaSuccess) return e;
     }
     for (size_t ri = 0; ri < p.rounds.size(); ri++)
         for (const Group &g : p.rounds[ri]) {
             const Work *w = p.d_work + g.off;
             const unsigned n = (unsigned)g.count;
+            const int si = (int)(ri % kRoundStreams);
             cudaStream_t st0 = st;
-            cudaStream_t st = (two && ri % 2 == 1) ? p.side : st0;
+            cudaStream_t st = (nstreams > 1 && si > 0) ? p.side[si - 1] : st0;
             time_begin(timer, st);
             if (g.fast) {
                 const int cnt = (int)g.count;
@@ -552,9 +564,9 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
             }
             if ((e = time_end(timer, g.stage, st)) != cudaSuccess) return e;
         }
-    if (two) {
-        if ((e = cudaEventRecord(p.ev_join, p.side)) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(st, p.ev_join, 0)) != cudaSuccess) return e;
+    for (int k = 0; k < nstreams - 1; k++) {
+        if ((e = cudaEventRecord(p.ev_join[k], p.side[k])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(st, p.ev_join[k], 0)) != cudaSuccess) return e;
     }
     if (kRK == 1) {
         time_begin(timer, st);

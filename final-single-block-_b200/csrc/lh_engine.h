@@ -76,8 +76,8 @@ struct Plan {
     size_t sm_col = 0;
     int ninst = 0;
     bool force_generic = false;
-    cudaStream_t side = nullptr;           // odd chunk rounds
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t side[kRoundStreams - 1] = {};  // rounds r % kRoundStreams != 0
+    cudaEvent_t ev_fork = nullptr, ev_join[kRoundStreams - 1] = {};
 };
 
 // Optional per-launch timing (kernel classes 0 z inverse, 1 x products,

@@ -5,9 +5,9 @@
 // the Ngal sizes of the usual grids.  One CTA per work item; the twiddle
 // table is copied into shared memory per CTA.
 //
-// Staging (per instance, inside I.S; two chunk rounds in flight use
-// disjoint halves):
-//   Sin  [cap+4][3][Mz][nxh]  z-inverse of u1, u3 and u2 on the y rows of
+// Staging (per instance, inside I.S; the kRoundStreams chunk rounds in
+// flight use disjoint shares):
+//   Sin  [cap+2*kRoundStreams][3][Mz][nxh]  z-inverse of u1, u3 and u2 on the y rows of
 //        a round's planes plus one halo row each side; x stays spectral.
 //   Sprod[cap][6][Mz][nxh]    the six products after the forward x
 //        transform, one slot per plane of a round.
@@ -50,7 +50,7 @@ __device__ __forceinline__ double2 *sin_field(const Inst &I, int p, int f)
 }
 __device__ __forceinline__ double2 *sprod_slot(const Inst &I, int s)
 {
-    return I.S + ((size_t)(I.chunk + 4) * 3 + (size_t)s * kNumProducts) * I.Mz * I.nxh;
+    return I.S + ((size_t)(I.chunk + 2 * kRoundStreams) * 3 + (size_t)s * kNumProducts) * I.Mz * I.nxh;
 }
 
 // ---------------------------------------------------------------------------
