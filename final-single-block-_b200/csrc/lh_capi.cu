@@ -80,6 +80,7 @@ extern "C" int lh_ctx_destroy(lh_ctx *c)
     if (c->graph) cudaGraphDestroy(c->graph);
     plan_free(c->plan);
     if (c->d_inst) cudaFree(c->d_inst);
+    if (c->d_spec) cudaFree(c->d_spec);
     instance_free(c->dev);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -228,6 +229,58 @@ extern "C" int lh_get_scalars(lh_ctx *c, double *t, double *dt, int *iter, doubl
     if (mpgx) *mpgx = sc[SC_MPGX];
     if (Qx) *Qx = sc[SC_QX];
     return LH_OK;
+}
+
+// ---- spectra of flagged steps (spectra.f90:7-66) ---------------------------
+extern "C" int lh_spectra_accumulate(lh_ctx *c)
+{
+    if (!c) return LH_EINVAL;
+    if (!c->have_state) return fail(c, LH_ESTATE, "no state uploaded");
+    const HostSetup &s = c->dev.hs;
+    const size_t bytes = spectra_doubles(s.nyu, s.nyv, s.nc) * sizeof(double);
+    if (!c->d_spec) {
+        CK(cudaMalloc(&c->d_spec, bytes), "alloc spectra");
+        CK(cudaMemsetAsync(c->d_spec, 0, bytes, c->st), "clear spectra");
+        c->spec_count = 0;
+    }
+    launch_spectra_accumulate(c->d_inst, c->d_spec, s.nyu, s.nc, c->st);
+    CK(cudaGetLastError(), "spectra launch");
+    c->spec_count++;
+    return LH_OK;
+}
+
+extern "C" int lh_spectra_reset(lh_ctx *c)
+{
+    if (!c) return LH_EINVAL;
+    if (c->d_spec) {
+        const HostSetup &s = c->dev.hs;
+        CK(cudaMemsetAsync(c->d_spec, 0, spectra_doubles(s.nyu, s.nyv, s.nc) * sizeof(double), c->st), "reset");
+    }
+    c->spec_count = 0;
+    return LH_OK;
+}
+
+extern "C" int lh_get_spectra(lh_ctx *c, int which, double *out, size_t cap, int *count)
+{
+    if (!c || which < 0 || which > 4) return fail(c, LH_EINVAL, "unknown spectrum");
+    const HostSetup &s = c->dev.hs;
+    const size_t nc = s.nc, nu = (size_t)(s.nyu + 2), nv = (size_t)(s.nyv + 2);
+    const size_t rows = which == 1 ? nv : which == 4 ? (size_t)s.nyu : nu;
+    const size_t off = which == 0 ? 0 : which == 1 ? nu : which == 2 ? nu + nv : which == 3 ? 2 * nu + nv : 3 * nu + nv;
+    const size_t n = rows * nc;
+    if (count) *count = c->spec_count;
+    if (!out) return (int)n;
+    if (cap < n) return fail(c, LH_EINVAL, "buffer too small");
+    std::vector<double> plane(n, 0.0);
+    if (c->d_spec) {
+        CK(cudaMemcpyAsync(plane.data(), c->d_spec + off * nc, n * sizeof(double), cudaMemcpyDeviceToHost, c->st),
+           "spectra download");
+        CK(cudaStreamSynchronize(c->st), "spectra download");
+    }
+    // plane-major (row, column) -> the reference's sp(j, column), j fastest
+    for (size_t j = 0; j < rows; j++)
+        for (size_t col = 0; col < nc; col++) out[col * rows + j] = plane[j * nc + col];
+    return (int)n;
 }
 
 extern "C" int lh_error_div(lh_ctx *c, double *err)

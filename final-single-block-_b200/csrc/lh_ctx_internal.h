@@ -15,5 +15,7 @@ struct lh_ctx {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     bool have_state = false;
+    double *d_spec = nullptr;  // spectra accumulators (lh_diag.cu), allocated on first use
+    int spec_count = 0;        // accumulations since the last reset
     std::string err;
 };

@@ -27,6 +27,10 @@ __global__ void k_lusolu(const Inst *__restrict__ insts, int grid, int kRK, doub
 __global__ void k_lusolp(const Inst *__restrict__ insts, double2 *x);
 __global__ void k_divmax(const Inst *__restrict__ insts, double *out);
 
+// on-device spectra of flagged steps (lh_diag.cu): accumulator doubles and launch
+size_t spectra_doubles(int nyu, int nyv, int nc);
+void launch_spectra_accumulate(const Inst *d_inst, double *sp, int nyu, int nc, cudaStream_t st);
+
 // raise (never lower) a kernel's dynamic shared-memory limit (lh_engine.cu)
 cudaError_t raise_smem_limit(const void *func, size_t bytes);
 

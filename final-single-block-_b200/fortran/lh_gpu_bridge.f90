@@ -85,6 +85,18 @@ module lh_gpu_bridge
       type(c_ptr), value :: ctx
       complex(c_double_complex) :: x(*)
     end function
+    integer(c_int) function lh_spectra_accumulate(ctx) bind(C, name="lh_spectra_accumulate")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function lh_get_spectra(ctx, which, out, cap, count) bind(C, name="lh_get_spectra")
+      import :: c_int, c_ptr, c_double, c_size_t
+      type(c_ptr), value       :: ctx
+      integer(c_int), value    :: which
+      real(c_double)           :: out(*)
+      integer(c_size_t), value :: cap
+      integer(c_int)           :: count
+    end function
   end interface
 
   type(c_ptr), save :: gpu_ctx = c_null_ptr
@@ -156,6 +168,23 @@ contains
   subroutine gpu_LUsolP(x)
     complex(8) :: x(*)
     call gpu_check(lh_lusolp(gpu_ctx, x), 'lh_lusolp')
+  end subroutine
+
+  ! spectra(u1,u2,u2_itp,u3,p,myid) at a flagged step (FOU3D.f90:137-141):
+  ! the accumulation stays on the device
+  subroutine gpu_spectra()
+    call gpu_check(lh_spectra_accumulate(gpu_ctx), 'lh_spectra_accumulate')
+  end subroutine
+
+  ! Bring the accumulated spectra back before write_spect (spectra.f90)
+  subroutine gpu_fetch_spectra(spU_, spV_, spW_, spUV_, spP_)
+    real(8) :: spU_(*), spV_(*), spW_(*), spUV_(*), spP_(*)
+    integer(c_int) :: n
+    n = lh_get_spectra(gpu_ctx, 0_c_int, spU_, huge(0_c_size_t), n)
+    n = lh_get_spectra(gpu_ctx, 1_c_int, spV_, huge(0_c_size_t), n)
+    n = lh_get_spectra(gpu_ctx, 2_c_int, spW_, huge(0_c_size_t), n)
+    n = lh_get_spectra(gpu_ctx, 3_c_int, spUV_, huge(0_c_size_t), n)
+    n = lh_get_spectra(gpu_ctx, 4_c_int, spP_, huge(0_c_size_t), n)
   end subroutine
 
   subroutine gpu_finalize()

@@ -29,6 +29,7 @@ EXPORTS = [
     "lh_lusolp", "lh_lusolu_noalloc", "lh_batch_create", "lh_batch_destroy", "lh_batch_last_error",
     "lh_instance_bytes", "lh_batch_add", "lh_batch_remove", "lh_batch_step",
     "lh_batch_download", "lh_batch_scalars", "lh_batch_count", "lh_batch_synchronize",
+    "lh_spectra_accumulate", "lh_spectra_reset", "lh_get_spectra",
 ]
 
 
@@ -141,6 +142,9 @@ def lib() -> ctypes.CDLL:
         "lh_batch_scalars": (i, [v, i, dp, dp, P(i)]),
         "lh_batch_count": (i, [v]),
         "lh_batch_synchronize": (i, [v]),
+        "lh_spectra_accumulate": (i, [v]),
+        "lh_spectra_reset": (i, [v]),
+        "lh_get_spectra": (i, [v, i, dp, sz, P(i)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -249,6 +253,28 @@ class Engine:
         e = ctypes.c_double()
         self._ck(self.L.lh_error_div(self.h, ctypes.byref(e)), "error_div")
         return e.value
+
+    # ---- spectra of flagged steps (spectra.f90) --------------------------
+    SPECTRA = ("spU", "spV", "spW", "spUV", "spP")
+
+    def spectra_accumulate(self):
+        """Add the current state's spectra terms (the reference's flagged-step call)."""
+        self._ck(self.L.lh_spectra_accumulate(self.h), "spectra_accumulate")
+
+    def spectra_reset(self):
+        self._ck(self.L.lh_spectra_reset(self.h), "spectra_reset")
+
+    def spectra(self) -> tuple[dict, int]:
+        """The accumulated spectra as {name: array[column, j]} and the count."""
+        out, cnt = {}, ctypes.c_int()
+        for w, name in enumerate(self.SPECTRA):
+            n = self.L.lh_get_spectra(self.h, w, None, 0, None)
+            if n < 0:
+                self._ck(n, "spectra")
+            a = np.zeros(n)
+            self._ck(min(0, self.L.lh_get_spectra(self.h, w, _dp(a), n, ctypes.byref(cnt))), "spectra")
+            out[name] = a.reshape(self.sizes.ncols, n // self.sizes.ncols)
+        return out, cnt.value
 
     def stream(self) -> int:
         s = ctypes.c_void_p()

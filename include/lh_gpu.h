@@ -116,6 +116,22 @@ int lh_profile(lh_ctx *ctx, int nsteps, double *ms, int *launches);
 /* max |div| after the last projection (error(), littleharsh.f90:370-409) */
 int lh_error_div(lh_ctx *ctx, double *err);
 
+/* ---- spectra of flagged steps: replace spectra() (spectra.f90:7-66), which
+ * nonlinear() calls every nstat steps at kRK = 1 (FOU3D.f90:76-81, 137-141).
+ * lh_spectra_accumulate adds the current state's terms into accumulators that
+ * stay on the device: spU/spV/spW += |u1|^2 / |u2|^2 / |u3|^2, spUV +=
+ * Re(u1 conj(u2 interpolated to the u rows by interp_v)), spP += |p|^2, per
+ * (y row, column).  Call it between steps where the reference's flag would be
+ * set; it is queued on the context's stream.  lh_get_spectra copies one of
+ * them out in the reference layout sp(j, column), rows fastest: which 0 spU
+ * and 2 spW and 3 spUV (rows 0..nyu+1), 1 spV (0..nyv+1), 4 spP (1..nyu);
+ * *count (optional) receives the accumulations since the last reset.  Returns
+ * the element count; out = NULL only queries it.  The first accumulation
+ * allocates the accumulators (5 x ncols x ny doubles). */
+int lh_spectra_accumulate(lh_ctx *ctx);
+int lh_spectra_reset(lh_ctx *ctx);
+int lh_get_spectra(lh_ctx *ctx, int which, double *out, size_t cap, int *count);
+
 /* ---- nonlinear-term intermediates of the last substep (parity) -------- */
 /* which: 0 Nu1 x/z part, 1 Nu2 x/z part, 2 Nu3 x/z part (FOU3D.f90:259-261
  * before the y-flux sum), 3 uv_f (j=0..nyv+1), 4 vv_c (j=0..nyu+1),

@@ -1252,6 +1252,34 @@ void lho_step(lho_ctx *c, int nsteps)
     }
 }
 
+/* spectra (spectra.f90:7-66): buildsp per field, buildspUV with u2_itp */
+void lho_spectra(lho_ctx *c, double *spU, double *spV, double *spW, double *spUV, double *spP)
+{
+    const int nc = c->ncols, lu = jlen(c, UGRID), lv = jlen(c, VGRID), lp = jlen(c, PGRID);
+    double *itp = (double *)malloc(sizeof(double) * 2 * (size_t)lu * nc);
+    interp_v(c, itp, c->u2);
+    for (int col = 1; col <= nc; col++) {
+        for (int j = 0; j < lu; j++) {
+            const size_t q = (size_t)(col - 1) * lu + j;
+            const double *a = CX(c->u1, 0, lu, j, col), *w = CX(c->u3, 0, lu, j, col), *v = CX(itp, 0, lu, j, col);
+            spU[q] = spU[q] + a[0] * a[0] + a[1] * a[1];
+            spW[q] = spW[q] + w[0] * w[0] + w[1] * w[1];
+            spUV[q] = spUV[q] + a[0] * v[0] + a[1] * v[1];
+        }
+        for (int j = 0; j < lv; j++) {
+            const size_t q = (size_t)(col - 1) * lv + j;
+            const double *a = CX(c->u2, 0, lv, j, col);
+            spV[q] = spV[q] + a[0] * a[0] + a[1] * a[1];
+        }
+        for (int j = 1; j <= lp; j++) {
+            const size_t q = (size_t)(col - 1) * lp + (j - 1);
+            const double *a = CX(c->p, 1, lp, j, col);
+            spP[q] = spP[q] + a[0] * a[0] + a[1] * a[1];
+        }
+    }
+    free(itp);
+}
+
 double lho_error_div(const lho_ctx *c)
 {
     size_t n = (size_t)jlen(c, PGRID) * c->ncols;

@@ -122,6 +122,13 @@ void lho_lusolp(const lho_ctx *c, double *x);
 /* max |div| over columns (littleharsh.f90:370-409) */
 double lho_error_div(const lho_ctx *c);
 
+/* spectra() at a flagged step (spectra.f90:7-66, called from nonlinear at
+ * FOU3D.f90:137-141): add the current state's terms into sp arrays in the
+ * reference layout sp(j, column), j fastest: spU, spW and spUV over u rows
+ * 0..nyu+1 (spUV with u2 interpolated to the u rows by interp_v), spV over
+ * v rows 0..nyv+1, spP over p rows 1..nyu. */
+void lho_spectra(lho_ctx *c, double *spU, double *spV, double *spW, double *spUV, double *spP);
+
 /* generic mode-count helpers for the 2-D (i,k) <-> plane map */
 int lho_column_i(const lho_ctx *c, int column);   /* 1-based column */
 int lho_column_k(const lho_ctx *c, int column);

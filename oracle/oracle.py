@@ -85,6 +85,7 @@ def lib(threaded: bool = False) -> ctypes.CDLL:
     L.lho_lusolp.argtypes = [v, dp]
     L.lho_error_div.restype = d
     L.lho_error_div.argtypes = [v]
+    L.lho_spectra.argtypes = [v, dp, dp, dp, dp, dp]
     L.lho_cfft_init.restype = i
     L.lho_rfft_init.restype = i
     _libs[threaded] = L
@@ -192,6 +193,16 @@ class Oracle:
 
     def error_div(self) -> float:
         return self.L.lho_error_div(self.h)
+
+    def spectra(self, acc: dict | None = None) -> dict:
+        """spectra() at a flagged step: add the current state's terms into acc
+        (new zero accumulators when None); arrays [column, j]."""
+        nc, nyu, nyv = self.ncols, self.nyu, self.nyv
+        if acc is None:
+            acc = {"spU": np.zeros((nc, nyu + 2)), "spV": np.zeros((nc, nyv + 2)), "spW": np.zeros((nc, nyu + 2)),
+                   "spUV": np.zeros((nc, nyu + 2)), "spP": np.zeros((nc, nyu))}
+        self.L.lho_spectra(self.h, *(_dp(acc[k]) for k in ("spU", "spV", "spW", "spUV", "spP")))
+        return acc
 
     # -- plane helpers ----------------------------------------------------
     def four_to_phys(self, plane: np.ndarray) -> np.ndarray:

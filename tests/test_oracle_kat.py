@@ -8,6 +8,8 @@
 * After a full RK3 step from the reference's 32x32x153 initial condition the
   projected field is divergence-free to round-off (error(), littleharsh.f90:
   370-409) and the time step follows the CFL rule (FOU3D.f90:290-303).
+* The spectra of flagged steps (spectra.f90:7-66) against a direct statement
+  of buildsp/buildspUV with interp_v.
 """
 import os
 
@@ -93,3 +95,31 @@ def test_one_step_from_reference_ic(golden_dir):
     assert o.scalar(1) == min(2.5 * dtv, 0.7 * o.scalar(7))
     s = o.state()
     assert np.all(np.isfinite(s["u1"])) and abs(s["u2"][:, 0]).max() == 0.0
+
+
+def test_oracle_spectra_follow_spectra_f90():
+    """lho_spectra adds, per (y row, column), |u1|^2, |u2|^2, |u3|^2, |p|^2 and
+    Re(u1) Re(u2i) + Im(u1) Im(u2i) with u2i = interp_v(u2) (spectra.f90:7-66,
+    FOU3D.f90:394-418); two accumulations of one state give twice the terms."""
+    from lh_b200 import Desc, grids, perturbed_laminar
+    d = Desc(Nx=16, Nz=16, ny=33, dt_mode=1, dt=1e-3)
+    yu, yv = grids(d)
+    o = O.Oracle(O.Config(Nx=16, Nz=16, ny=33, dt_mode=O.DT_FIXED, dt_fixed=1e-3))
+    o.load_state(*perturbed_laminar(d, 3, yu, yv))
+    o.step(1)
+    st = o.state()
+    acc = o.spectra(o.spectra())
+    u1, u2, u3, p = st["u1"], st["u2"], st["u3"], st["p"]
+    nyu = d.nyu
+    ui = np.zeros_like(u1)
+    for j in range(1, nyu + 1):
+        ui[:, j] = ((yu[j] - yv[j - 1]) * u2[:, j] + (yv[j] - yu[j]) * u2[:, j - 1]) / (yv[j] - yv[j - 1])
+    g1 = (yu[0] - yu[1]) / (yv[0] - yu[1])
+    g2 = (yu[nyu + 1] - yu[nyu]) / (yv[nyu] - yu[nyu])
+    ui[:, 0] = g1 * (u2[:, 0] - ui[:, 1]) + ui[:, 1]
+    ui[:, -1] = g2 * (u2[:, -1] - ui[:, -2]) + ui[:, -2]
+    ref = {"spU": 2 * abs(u1) ** 2, "spV": 2 * abs(u2) ** 2, "spW": 2 * abs(u3) ** 2,
+           "spUV": 2 * (u1.real * ui.real + u1.imag * ui.imag), "spP": 2 * abs(p) ** 2}
+    for k, r in ref.items():
+        assert acc[k].shape == r.shape, k
+        assert np.max(abs(acc[k] - r)) <= 1e-14 * np.max(abs(r)), k
