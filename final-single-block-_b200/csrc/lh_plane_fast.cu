@@ -44,6 +44,20 @@
 
 namespace lh {
 
+// Outer twiddles W^(r k1), k1 = 1.., of a two-pass transform by the
+// recurrence W^(r k1) = W^(r (k1-1)) W^r from one table entry, which keeps the
+// per-point table reads out of the shared-memory pipe (the kernels' busiest
+// unit); the recurrence's rounding stays within a few ulp for k1 <= 24.
+struct TwStep {
+    double2 w1, wk;
+    __device__ explicit TwStep(const double2 *tw, int r) : w1(tw[r]), wk(make_double2(1.0, 0.0)) {}
+    __device__ __forceinline__ double2 next()
+    {
+        wk = make_double2(wk.x * w1.x - wk.y * w1.y, wk.x * w1.y + wk.y * w1.x);
+        return wk;
+    }
+};
+
 __device__ __forceinline__ double2 *sin_field(const Inst &I, int p, int f)
 {
     return I.S + ((size_t)p * 3 + f) * I.Mz * I.nxh;
@@ -87,10 +101,11 @@ __global__ void __launch_bounds__(LH_ZINV_T, LH_ZINV_B) k_zinv_f(const Inst *__r
                 a[n1] = (kr >= 0 && ok) ? src[kr * nxh + i] : make_double2(0.0, 0.0);
             }
             DFT<N1, +1, NZ>::run(a, tw);
+            TwStep ts(tw, r);
 #pragma unroll
             for (int k1 = 0; k1 < N1; k1++) {
                 double2 z = a[k1];
-                if (k1 > 0 && r > 0) z = twiddle<+1>(tw[r * k1], z);
+                if (k1 > 0) z = twiddle<+1>(ts.next(), z);
                 T[(k1 * N2 + r) * cb + v] = z;
             }
         }
@@ -127,7 +142,6 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
     if ((int)blockIdx.x >= count) return;
     load_table(tw, insts[work[blockIdx.x].inst].twx, NX);  // depends on Mx only
     const int t = threadIdx.x, nv = 3 * rb, v = t % nv, r = t / nv;
-    const int pr = v / rb, rr = v % rb;
     constexpr int nxh = NX / 3 + 1;  // Nx/2 + 1 with Mx = 3 Nx / 2
     const FastDiv by_rb(rb), by_nv(nv);
     {
@@ -144,57 +158,55 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
         const double w0u = (I.yv[j] - I.yu[j]) * dnu, w1u = (I.yu[j + 1] - I.yv[j]) * dnu;
         double2 *S = sprod_slot(I, w.slot);
         __syncthreads();  // table loaded / buf free
-        // (0) coalesced gather of the 6 fields x rb rows x (Nx/2+1) modes: in[f][rr][k]
-        double2 *in = buf;
-        for (int e = t; e < kNumProducts * rb * nxh; e += blockDim.x) {
-            const int fr = e / nxh, k = e - fr * nxh, f = by_rb.div(fr), r2 = by_rb.mod(fr, f);
+        // (0) coalesced gather of the rows (k fastest) straight into the packed
+        // complex vectors of the inverse transform, z[n][v] (v = pair*rb + row):
+        // z = A + iB for the two real rows A, B of a pair, Hermitian-extended,
+        // Im of mode 0 dropped (rft_buff.f:78-81), zero between the retained
+        // modes
+        for (int e = t; e < 3 * rb * nxh; e += blockDim.x) {
+            const int fr = e / nxh, k = e - fr * nxh, p2 = by_rb.div(fr), r2 = by_rb.mod(fr, p2);
             const int q = q0 + r2;
-            double2 val = make_double2(0.0, 0.0);
+            double2 A = make_double2(0.0, 0.0), B = A;
             if (q < Mz) {
                 const size_t o = (size_t)q * nxh + k;
-                if (f == 0) val = u1j[o];
-                else if (f == 2) val = u3j[o];
-                else if (f == 4) val = vj[o];
-                else if (f == 1) {
+                if (p2 == 0) {  // (u1, u3) at the centre
+                    A = u1j[o];
+                    B = u3j[o];
+                } else if (p2 == 1) {  // (u2 at the centre, u2 at the face)
                     const double2 x0 = vj[o], x1 = vjm[o];
-                    val = make_double2(w0v * x0.x + w1v * x1.x, w0v * x0.y + w1v * x1.y);
-                } else {
-                    const double2 x0 = f == 3 ? u1p[o] : u3p[o], x1 = f == 3 ? u1j[o] : u3j[o];
-                    val = make_double2(w0u * x0.x + w1u * x1.x, w0u * x0.y + w1u * x1.y);
+                    A = make_double2(w0v * x0.x + w1v * x1.x, w0v * x0.y + w1v * x1.y);
+                    B = x0;
+                } else {  // (u1, u3) at the face
+                    const double2 a0 = u1p[o], a1 = u1j[o], b0 = u3p[o], b1 = u3j[o];
+                    A = make_double2(w0u * a0.x + w1u * a1.x, w0u * a0.y + w1u * a1.y);
+                    B = make_double2(w0u * b0.x + w1u * b1.x, w0u * b0.y + w1u * b1.y);
                 }
             }
-            in[e] = val;
+            const int vv = p2 * rb + r2;
+            if (k == 0) {
+                buf[vv] = make_double2(A.x, B.x);
+            } else {
+                buf[k * nv + vv] = make_double2(A.x - B.y, A.y + B.x);
+                buf[(NX - k) * nv + vv] = make_double2(A.x + B.y, B.x - A.y);
+            }
         }
+        for (int e = t; e < (NX - 2 * nxh + 1) * nv; e += blockDim.x) buf[nxh * nv + e] = make_double2(0.0, 0.0);
         __syncthreads();
-        // (1) inverse pass 1 on the Hermitian extension of two half spectra
+        // (1) inverse pass 1: lane r < N2 holds n = r + N2*n1
         {
             double2 a[N1];
             if (r < N2) {
-                const int fa = pr == 0 ? 0 : (pr == 1 ? 1 : 3), fb = pr == 0 ? 2 : (pr == 1 ? 4 : 5);
-                const double2 *A = in + (fa * rb + rr) * nxh, *B = in + (fb * rb + rr) * nxh;
 #pragma unroll
-                for (int n1 = 0; n1 < N1; n1++) {
-                    const int n = r + N2 * n1;
-                    double2 z = make_double2(0.0, 0.0);
-                    if (n == 0) {
-                        z = make_double2(A[0].x, B[0].x);  // Im of mode 0 dropped (rft_buff.f:78-81)
-                    } else if (n < nxh) {
-                        const double2 x = A[n], y = B[n];
-                        z = make_double2(x.x - y.y, x.y + y.x);
-                    } else if (NX - n < nxh) {
-                        const double2 x = A[NX - n], y = B[NX - n];
-                        z = make_double2(x.x + y.y, y.x - x.y);
-                    }
-                    a[n1] = z;
-                }
+                for (int n1 = 0; n1 < N1; n1++) a[n1] = buf[(r + N2 * n1) * nv + v];
             }
             __syncthreads();
             if (r < N2) {
                 DFT<N1, +1, NX>::run(a, tw);
+                TwStep ts(tw, r);
 #pragma unroll
                 for (int k1 = 0; k1 < N1; k1++) {
                     double2 z = a[k1];
-                    if (k1 > 0 && r > 0) z = twiddle<+1>(tw[r * k1], z);
+                    if (k1 > 0) z = twiddle<+1>(ts.next(), z);
                     buf[(k1 * N2 + r) * nv + v] = z;
                 }
             }
@@ -262,10 +274,11 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
             }
             __syncthreads();
             if (r < N2) {
+                TwStep ts(tw, r);
 #pragma unroll
                 for (int k1 = 0; k1 < N1; k1++) {
                     double2 z = a[k1];
-                    if (k1 > 0 && r > 0) z = twiddle<-1>(tw[r * k1], z);
+                    if (k1 > 0) z = twiddle<-1>(ts.next(), z);
                     buf[(k1 * N2 + r) * nv + v] = z;
                 }
             }
@@ -341,10 +354,11 @@ __global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_f(const Inst *__r
             for (int n1 = 0; n1 < N1; n1++)
                 a[n1] = ok ? S[((size_t)g * NZ + r + N2 * n1) * nxh + i] : make_double2(0.0, 0.0);
             DFT<N1, -1, NZ>::run(a, tw);
+            TwStep ts(tw, r);
 #pragma unroll
             for (int k1 = 0; k1 < N1; k1++) {
                 double2 z = a[k1];
-                if (k1 > 0 && r > 0) z = twiddle<-1>(tw[r * k1], z);
+                if (k1 > 0) z = twiddle<-1>(ts.next(), z);
                 T[(k1 * N2 + r) * nv + v] = z;
             }
         }
