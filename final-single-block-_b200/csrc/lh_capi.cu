@@ -81,6 +81,7 @@ extern "C" int lh_ctx_destroy(lh_ctx *c)
     plan_free(c->plan);
     if (c->d_inst) cudaFree(c->d_inst);
     if (c->d_spec) cudaFree(c->d_spec);
+    if (c->d_stats) cudaFree(c->d_stats);
     instance_free(c->dev);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -280,6 +281,48 @@ extern "C" int lh_get_spectra(lh_ctx *c, int which, double *out, size_t cap, int
     // plane-major (row, column) -> the reference's sp(j, column), j fastest
     for (size_t j = 0; j < rows; j++)
         for (size_t col = 0; col < nc; col++) out[col * rows + j] = plane[j * nc + col];
+    return (int)n;
+}
+
+// ---- stats of flagged output steps (stats.f90:1-97) ------------------------
+extern "C" int lh_stats_accumulate(lh_ctx *c)
+{
+    if (!c) return LH_EINVAL;
+    if (!c->have_state) return fail(c, LH_ESTATE, "no state uploaded");
+    const HostSetup &s = c->dev.hs;
+    const size_t bytes = stats_doubles(s.nyu) * sizeof(double);
+    if (!c->d_stats) {
+        CK(cudaMalloc(&c->d_stats, bytes), "alloc stats");
+        CK(cudaMemsetAsync(c->d_stats, 0, bytes, c->st), "clear stats");
+        c->stats_count = 0;
+    }
+    launch_stats_accumulate(c->d_inst, c->d_stats, s.nyu, c->st);
+    CK(cudaGetLastError(), "stats launch");
+    c->stats_count++;
+    return LH_OK;
+}
+
+extern "C" int lh_stats_reset(lh_ctx *c)
+{
+    if (!c) return LH_EINVAL;
+    if (c->d_stats) CK(cudaMemsetAsync(c->d_stats, 0, stats_doubles(c->dev.hs.nyu) * sizeof(double), c->st), "reset");
+    c->stats_count = 0;
+    return LH_OK;
+}
+
+extern "C" int lh_get_stats(lh_ctx *c, double *out, size_t cap, int *count)
+{
+    if (!c) return LH_EINVAL;
+    const size_t n = stats_doubles(c->dev.hs.nyu);
+    if (count) *count = c->stats_count;
+    if (!out) return (int)n;
+    if (cap < n) return fail(c, LH_EINVAL, "buffer too small");
+    if (!c->d_stats) {
+        memset(out, 0, n * sizeof(double));
+        return (int)n;
+    }
+    CK(cudaMemcpyAsync(out, c->d_stats, n * sizeof(double), cudaMemcpyDeviceToHost, c->st), "stats download");
+    CK(cudaStreamSynchronize(c->st), "stats download");
     return (int)n;
 }
 

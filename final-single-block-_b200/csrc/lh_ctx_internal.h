@@ -17,5 +17,7 @@ struct lh_ctx {
     bool have_state = false;
     double *d_spec = nullptr;  // spectra accumulators (lh_diag.cu), allocated on first use
     int spec_count = 0;        // accumulations since the last reset
+    double *d_stats = nullptr; // stats accumulators (lh_diag.cu), allocated on first use
+    int stats_count = 0;
     std::string err;
 };

@@ -30,6 +30,8 @@ __global__ void k_divmax(const Inst *__restrict__ insts, double *out);
 // on-device spectra of flagged steps (lh_diag.cu): accumulator doubles and launch
 size_t spectra_doubles(int nyu, int nyv, int nc);
 void launch_spectra_accumulate(const Inst *d_inst, double *sp, int nyu, int nc, cudaStream_t st);
+size_t stats_doubles(int nyu);
+void launch_stats_accumulate(const Inst *d_inst, double *acc, int nyu, cudaStream_t st);
 
 // raise (never lower) a kernel's dynamic shared-memory limit (lh_engine.cu)
 cudaError_t raise_smem_limit(const void *func, size_t bytes);

@@ -89,6 +89,17 @@ module lh_gpu_bridge
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
     end function
+    integer(c_int) function lh_stats_accumulate(ctx) bind(C, name="lh_stats_accumulate")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function lh_get_stats(ctx, out, cap, count) bind(C, name="lh_get_stats")
+      import :: c_int, c_ptr, c_double, c_size_t
+      type(c_ptr), value       :: ctx
+      real(c_double)           :: out(*)
+      integer(c_size_t), value :: cap
+      integer(c_int)           :: count
+    end function
     integer(c_int) function lh_get_spectra(ctx, which, out, cap, count) bind(C, name="lh_get_spectra")
       import :: c_int, c_ptr, c_double, c_size_t
       type(c_ptr), value       :: ctx
@@ -185,6 +196,21 @@ contains
     n = lh_get_spectra(gpu_ctx, 2_c_int, spW_, huge(0_c_size_t), n)
     n = lh_get_spectra(gpu_ctx, 3_c_int, spUV_, huge(0_c_size_t), n)
     n = lh_get_spectra(gpu_ctx, 4_c_int, spP_, huge(0_c_size_t), n)
+  end subroutine
+
+  ! stats(myid,status,ierr) where flagst and flagwr are both set (FOU3D.f90:340)
+  subroutine gpu_stats()
+    call gpu_check(lh_stats_accumulate(gpu_ctx), 'lh_stats_accumulate')
+  end subroutine
+
+  ! The nine plane sums acc(0:nyu+1, 9) = Um U2m Vm V2m Wm W2m UVm UWm VWm,
+  ! with the number of accumulations (istat)
+  subroutine gpu_fetch_stats(acc, nstat_done)
+    real(8) :: acc(*)
+    integer :: nstat_done
+    integer(c_int) :: n, cnt
+    n = lh_get_stats(gpu_ctx, acc, huge(0_c_size_t), cnt)
+    nstat_done = cnt
   end subroutine
 
   subroutine gpu_finalize()

@@ -30,6 +30,7 @@ EXPORTS = [
     "lh_instance_bytes", "lh_batch_add", "lh_batch_remove", "lh_batch_step",
     "lh_batch_download", "lh_batch_scalars", "lh_batch_count", "lh_batch_synchronize",
     "lh_spectra_accumulate", "lh_spectra_reset", "lh_get_spectra",
+    "lh_stats_accumulate", "lh_stats_reset", "lh_get_stats",
 ]
 
 
@@ -145,6 +146,9 @@ def lib() -> ctypes.CDLL:
         "lh_spectra_accumulate": (i, [v]),
         "lh_spectra_reset": (i, [v]),
         "lh_get_spectra": (i, [v, i, dp, sz, P(i)]),
+        "lh_stats_accumulate": (i, [v]),
+        "lh_stats_reset": (i, [v]),
+        "lh_get_stats": (i, [v, dp, sz, P(i)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -275,6 +279,24 @@ class Engine:
             self._ck(min(0, self.L.lh_get_spectra(self.h, w, _dp(a), n, ctypes.byref(cnt))), "spectra")
             out[name] = a.reshape(self.sizes.ncols, n // self.sizes.ncols)
         return out, cnt.value
+
+    # ---- stats of flagged output steps (stats.f90) ----------------------
+    STATS = ("Um", "U2m", "Vm", "V2m", "Wm", "W2m", "UVm", "UWm", "VWm")
+
+    def stats_accumulate(self):
+        self._ck(self.L.lh_stats_accumulate(self.h), "stats_accumulate")
+
+    def stats_reset(self):
+        self._ck(self.L.lh_stats_reset(self.h), "stats_reset")
+
+    def stats(self) -> tuple[np.ndarray, int]:
+        """The nine plane sums as array[9, nyu+2] and the accumulation count."""
+        n = self.L.lh_get_stats(self.h, None, 0, None)
+        if n < 0:
+            self._ck(n, "stats")
+        a, cnt = np.zeros(n), ctypes.c_int()
+        self._ck(min(0, self.L.lh_get_stats(self.h, _dp(a), n, ctypes.byref(cnt))), "stats")
+        return a.reshape(9, n // 9), cnt.value
 
     def stream(self) -> int:
         s = ctypes.c_void_p()

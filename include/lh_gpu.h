@@ -132,6 +132,20 @@ int lh_spectra_accumulate(lh_ctx *ctx);
 int lh_spectra_reset(lh_ctx *ctx);
 int lh_get_spectra(lh_ctx *ctx, int which, double *out, size_t cap, int *count);
 
+/* ---- stats of flagged output steps: replace stats() (stats.f90:1-97),
+ * called from nonlinear() when both the stats and the output flags are set
+ * (FOU3D.f90:300-341).  At that point the reference's plane arrays hold the
+ * spectral coefficients placed by modes_to_planes_UVP, so its "plane sums"
+ * run over those: lh_stats_accumulate adds, per plane j = 0..nyu+1, the nine
+ * sums Um, U2m, Vm, V2m, Wm, W2m, UVm (u1 x u2 interpolated to the u rows),
+ * UWm, VWm (u2 x u3 interpolated to the v rows) in the reference's order.
+ * lh_get_stats copies out acc[9][nyu+2] and the count of accumulations.
+ * Not built: Pm/P2m (the reference reads ppPL before refreshing it, i.e. the
+ * pressure of the previous output step) and wxm/wx2m (omega_x). */
+int lh_stats_accumulate(lh_ctx *ctx);
+int lh_stats_reset(lh_ctx *ctx);
+int lh_get_stats(lh_ctx *ctx, double *out, size_t cap, int *count);
+
 /* ---- nonlinear-term intermediates of the last substep (parity) -------- */
 /* which: 0 Nu1 x/z part, 1 Nu2 x/z part, 2 Nu3 x/z part (FOU3D.f90:259-261
  * before the y-flux sum), 3 uv_f (j=0..nyv+1), 4 vv_c (j=0..nyu+1),

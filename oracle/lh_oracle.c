@@ -1280,6 +1280,55 @@ void lho_spectra(lho_ctx *c, double *spU, double *spV, double *spW, double *spUV
     free(itp);
 }
 
+/* stats (stats.f90:1-97) at a flagged output step: the sums run over the
+ * plane arrays as nonlinear() holds them when stats is called (FOU3D.f90:
+ * 300-341), i.e. after modes_to_planes_UVP and before ops_in_planes2 -- the
+ * spectral coefficients in the plane layout, entries i = 1..igal-2, rows
+ * k = 1..kgal, planes limPL_incw (0..nyu+1 on every grid at one rank).
+ * acc[q*(nyu+2) + j]: q 0 Um, 1 U2m, 2 Vm, 3 V2m, 4 Wm, 5 W2m, 6 UVm (u1 x
+ * u2PL_itp), 7 UWm, 8 VWm (u2 x u3PL_itp). */
+void lho_stats(lho_ctx *c, double *acc)
+{
+    const int nyu = c->nyu, nc = c->ncols, lu = jlen(c, UGRID), lv = jlen(c, VGRID);
+    const size_t plane = (size_t)c->igal * c->kgal, npl = (size_t)nyu + 2;
+    double *P1 = zalloc(plane * npl), *P2 = zalloc(plane * npl), *P3 = zalloc(plane * npl);
+    double *P2i = zalloc(plane * npl), *P3i = zalloc(plane * npl);
+    double *u2i = zalloc(2 * (size_t)lu * nc), *u3i = zalloc(2 * (size_t)lv * nc);
+    interp_v(c, u2i, c->u2);
+    interp_u(c, u3i, c->u3);
+    modes_to_planes(c, P1, c->u1, UGRID);
+    modes_to_planes(c, P2, c->u2, VGRID);
+    modes_to_planes(c, P3, c->u3, UGRID);
+    modes_to_planes(c, P2i, u2i, UGRID);
+    modes_to_planes(c, P3i, u3i, VGRID);
+    for (int j = 0; j <= nyu + 1; j++) {
+        double *Um = acc + 0 * npl + j, *U2m = acc + 1 * npl + j, *Vm = acc + 2 * npl + j, *V2m = acc + 3 * npl + j;
+        double *Wm = acc + 4 * npl + j, *W2m = acc + 5 * npl + j, *UVm = acc + 6 * npl + j, *UWm = acc + 7 * npl + j;
+        double *VWm = acc + 8 * npl + j;
+        for (int k = 1; k <= c->kgal; k++)
+            for (int i = 1; i <= c->igal - 2; i++) {
+                const double a = *PL(c, P1, i, k, j), v = *PL(c, P2, i, k, j), w = *PL(c, P3, i, k, j);
+                const double vi = *PL(c, P2i, i, k, j), wi = *PL(c, P3i, i, k, j);
+                *Um = *Um + a;
+                *U2m = *U2m + a * a;
+                *Vm = *Vm + v;
+                *V2m = *V2m + v * v;
+                *Wm = *Wm + w;
+                *W2m = *W2m + w * w;
+                *UVm = *UVm + a * vi;
+                *UWm = *UWm + a * w;
+                *VWm = *VWm + v * wi;
+            }
+    }
+    free(P1);
+    free(P2);
+    free(P3);
+    free(P2i);
+    free(P3i);
+    free(u2i);
+    free(u3i);
+}
+
 double lho_error_div(const lho_ctx *c)
 {
     size_t n = (size_t)jlen(c, PGRID) * c->ncols;

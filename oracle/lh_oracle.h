@@ -129,6 +129,12 @@ double lho_error_div(const lho_ctx *c);
  * v rows 0..nyv+1, spP over p rows 1..nyu. */
 void lho_spectra(lho_ctx *c, double *spU, double *spV, double *spW, double *spUV, double *spP);
 
+/* stats (stats.f90:1-97): add the plane sums of the current state into
+ * acc[9][nyu+2] (Um U2m Vm V2m Wm W2m UVm UWm VWm over planes 0..nyu+1); the
+ * planes hold the spectral coefficients in the plane layout, as they do in
+ * nonlinear() when stats is called (FOU3D.f90:300-341). */
+void lho_stats(lho_ctx *c, double *acc);
+
 /* generic mode-count helpers for the 2-D (i,k) <-> plane map */
 int lho_column_i(const lho_ctx *c, int column);   /* 1-based column */
 int lho_column_k(const lho_ctx *c, int column);

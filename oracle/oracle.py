@@ -86,6 +86,7 @@ def lib(threaded: bool = False) -> ctypes.CDLL:
     L.lho_error_div.restype = d
     L.lho_error_div.argtypes = [v]
     L.lho_spectra.argtypes = [v, dp, dp, dp, dp, dp]
+    L.lho_stats.argtypes = [v, dp]
     L.lho_cfft_init.restype = i
     L.lho_rfft_init.restype = i
     _libs[threaded] = L
@@ -193,6 +194,15 @@ class Oracle:
 
     def error_div(self) -> float:
         return self.L.lho_error_div(self.h)
+
+    STATS = ("Um", "U2m", "Vm", "V2m", "Wm", "W2m", "UVm", "UWm", "VWm")
+
+    def stats(self, acc: np.ndarray | None = None) -> np.ndarray:
+        """stats() at a flagged output step: add into acc[9, nyu+2] (new zeros when None)."""
+        if acc is None:
+            acc = np.zeros((9, self.nyu + 2))
+        self.L.lho_stats(self.h, _dp(acc))
+        return acc
 
     def spectra(self, acc: dict | None = None) -> dict:
         """spectra() at a flagged step: add the current state's terms into acc

@@ -123,3 +123,25 @@ def test_oracle_spectra_follow_spectra_f90():
     for k, r in ref.items():
         assert acc[k].shape == r.shape, k
         assert np.max(abs(acc[k] - r)) <= 1e-14 * np.max(abs(r)), k
+
+
+def test_oracle_stats_follow_stats_f90():
+    """lho_stats sums, per plane, the spectral coefficients the plane arrays
+    hold when stats() runs (re and im entries): Um = sum(Re + Im), U2m =
+    sum |u1|^2, V2m = sum |u2|^2 over the v planes (zero above nyv+1)."""
+    from lh_b200 import Desc, grids, perturbed_laminar
+    d = Desc(Nx=16, Nz=16, ny=33, dt_mode=1, dt=1e-3)
+    yu, yv = grids(d)
+    o = O.Oracle(O.Config(Nx=16, Nz=16, ny=33, dt_mode=O.DT_FIXED, dt_fixed=1e-3))
+    o.load_state(*perturbed_laminar(d, 3, yu, yv))
+    o.step(1)
+    acc = o.stats()
+    st = o.state()
+    u1, u2, u3 = st["u1"], st["u2"], st["u3"]
+    scale = np.max(abs(u1)) ** 2 * u1.shape[0]
+    assert np.max(abs(acc[0] - (u1.real + u1.imag).sum(0))) <= 1e-13 * scale
+    assert np.max(abs(acc[1] - (abs(u1) ** 2).sum(0))) <= 1e-13 * scale
+    v2 = np.zeros(d.nyu + 2)
+    v2[:d.nyv + 2] = (abs(u2) ** 2).sum(0)
+    assert np.max(abs(acc[3] - v2)) <= 1e-13 * scale
+    assert np.max(abs(acc[7] - (u1.real * u3.real + u1.imag * u3.imag).sum(0))) <= 1e-13 * scale
