@@ -82,6 +82,7 @@ extern "C" int lh_ctx_destroy(lh_ctx *c)
     if (c->d_inst) cudaFree(c->d_inst);
     if (c->d_spec) cudaFree(c->d_spec);
     if (c->d_stats) cudaFree(c->d_stats);
+    stats_release(c->stats_scr);
     instance_free(c->dev);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -296,10 +297,33 @@ extern "C" int lh_stats_accumulate(lh_ctx *c)
         CK(cudaMemsetAsync(c->d_stats, 0, bytes, c->st), "clear stats");
         c->stats_count = 0;
     }
-    launch_stats_accumulate(c->d_inst, c->d_stats, s.nyu, c->st);
-    CK(cudaGetLastError(), "stats launch");
+    CK(launch_stats_accumulate(c->d_inst, s, c->stats_scr.pp, c->d_stats, c->st), "stats launch");
     c->stats_count++;
     return LH_OK;
+}
+
+extern "C" int lh_pressure_snapshot(lh_ctx *c)
+{
+    if (!c) return LH_EINVAL;
+    if (!c->have_state) return fail(c, LH_ESTATE, "no state uploaded");
+    const HostSetup &s = c->dev.hs;
+    const size_t bytes = (size_t)s.nyu * s.nc * sizeof(double2);
+    if (!c->stats_scr.pp) CK(cudaMalloc(&c->stats_scr.pp, bytes), "alloc pressure snapshot");
+    CK(cudaMemcpyAsync(c->stats_scr.pp, c->dev.inst.P, bytes, cudaMemcpyDeviceToDevice, c->st), "pressure snapshot");
+    return LH_OK;
+}
+
+extern "C" int lh_omega_x(lh_ctx *c, double *out, size_t cap)
+{
+    if (!c) return LH_EINVAL;
+    const HostSetup &s = c->dev.hs;
+    const size_t n = (size_t)(s.nyu + 2) * s.Nz * (s.Nx + 2);
+    if (!out) return (int)n;
+    if (!c->have_state) return fail(c, LH_ESTATE, "no state uploaded");
+    if (cap < n) return fail(c, LH_EINVAL, "buffer too small");
+    CK(stats_prepare(c->dev, c->stats_scr), "stats scratch");
+    CK(omega_x_planes(c->d_inst, s, c->stats_scr, out, c->st), "omega_x");
+    return (int)n;
 }
 
 extern "C" int lh_stats_reset(lh_ctx *c)
@@ -381,7 +405,7 @@ static int plane_transform(lh_ctx *c, double *planes, int nplanes, int sgn)
         if (sgn > 0) {
             raise_smem_limit((const void *)k_plane_z_inv, smz);
             raise_smem_limit((const void *)k_plane_x_inv, smx);
-            k_plane_z_inv<<<nplanes * nbz, thr, smz, c->st>>>(c->d_inst, d, bc);
+            k_plane_z_inv<<<nplanes * nbz, thr, smz, c->st>>>(c->d_inst, d, bc, 1);
             k_plane_x_inv<<<nplanes * nbx, thr, smx, c->st>>>(c->d_inst, d, br);
         } else {
             raise_smem_limit((const void *)k_plane_z_fwd, smz);

@@ -19,5 +19,6 @@ struct lh_ctx {
     int spec_count = 0;        // accumulations since the last reset
     double *d_stats = nullptr; // stats accumulators (lh_diag.cu), allocated on first use
     int stats_count = 0;
+    lh::StatsScratch stats_scr;  // stats transform scratch and pressure snapshot
     std::string err;
 };

@@ -53,6 +53,27 @@ cudaError_t instance_upload(DevInstance &d, const double *u1, const double *u2, 
 cudaError_t instance_download(DevInstance &d, double *u1, double *u2, double *u3, double *p, cudaStream_t st);
 cudaError_t download_field(const DevInstance &d, const double2 *src, int len, double *dst, cudaStream_t st);
 
+// Device resources of the diagnostics (lh_diag.cu): the pressure snapshot the
+// stats read, and the transform scratch of omega_x, allocated on first use.
+struct StatsScratch {
+    double *planes = nullptr;  // omega_x transform scratch
+    size_t bytes = 0;
+    int chunk_n = 0;           // omega_x planes per pass (Nspec-sized)
+    Inst *d_inst_n = nullptr;  // instance record with the Nspec transform sizes and tables
+    double2 *tw_n = nullptr;   // its twiddles: z (Nz), then x (Nx)
+    double2 *pp = nullptr;     // pressure snapshot (rows 1..nyu), from the first snapshot on
+};
+cudaError_t stats_prepare(const DevInstance &d, StatsScratch &s);
+void stats_release(StatsScratch &s);
+size_t stats_doubles(int nyu);
+// Adds the current state's stats into acc[13][nyu+2]; pp (the pressure
+// snapshot) may be null.
+cudaError_t launch_stats_accumulate(const Inst *d_inst, const HostSetup &hs, const double2 *pp, double *acc,
+                                    cudaStream_t st);
+// omega_x of the current state into host out[(nyu+2)][Nz][Nx+2] (synchronous).
+cudaError_t omega_x_planes(const Inst *d_inst, const HostSetup &hs, const StatsScratch &s, double *out,
+                           cudaStream_t st);
+
 // One kernel launch of the plane pipeline: all work items of one stage for
 // the instances of one size class in one chunk round.
 struct Group {

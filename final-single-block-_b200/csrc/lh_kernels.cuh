@@ -12,7 +12,7 @@ size_t column_smem_bytes(int max_nyu);  // ring + staged y metrics
 __global__ void k_zinv(const Inst *__restrict__ insts, const Work *__restrict__ work, int bc);
 __global__ void k_xprod(const Inst *__restrict__ insts, const Work *__restrict__ work, int br, int want_max);
 __global__ void k_zfwd(const Inst *__restrict__ insts, const Work *__restrict__ work, int bc);
-__global__ void k_plane_z_inv(const Inst *__restrict__ insts, double *planes, int bc);
+__global__ void k_plane_z_inv(const Inst *__restrict__ insts, double *planes, int bc, int zero_row);
 __global__ void k_plane_z_fwd(const Inst *__restrict__ insts, double *planes, int bc);
 __global__ void k_plane_x_inv(const Inst *__restrict__ insts, double *planes, int br);
 __global__ void k_plane_x_fwd(const Inst *__restrict__ insts, double *planes, int br);
@@ -27,11 +27,10 @@ __global__ void k_lusolu(const Inst *__restrict__ insts, int grid, int kRK, doub
 __global__ void k_lusolp(const Inst *__restrict__ insts, double2 *x);
 __global__ void k_divmax(const Inst *__restrict__ insts, double *out);
 
-// on-device spectra of flagged steps (lh_diag.cu): accumulator doubles and launch
+// on-device spectra of flagged steps (lh_diag.cu): accumulator doubles and launch;
+// the plane stats are declared in lh_engine.h
 size_t spectra_doubles(int nyu, int nyv, int nc);
 void launch_spectra_accumulate(const Inst *d_inst, double *sp, int nyu, int nc, cudaStream_t st);
-size_t stats_doubles(int nyu);
-void launch_stats_accumulate(const Inst *d_inst, double *acc, int nyu, cudaStream_t st);
 
 // raise (never lower) a kernel's dynamic shared-memory limit (lh_engine.cu)
 cudaError_t raise_smem_limit(const void *func, size_t bytes);

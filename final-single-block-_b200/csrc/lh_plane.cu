@@ -262,9 +262,13 @@ __global__ void k_zfwd(const Inst *__restrict__ insts, const Work *__restrict__ 
 // four_to_phys/phys_to_four entry points.  Planes are real (Mx+2) x Mz
 // arrays, x fastest, (re, im) pairs for spectral columns.
 
-// z transform of the columns i = 0..Nx/2 of a plane (cft with m = (Nx+2)/2)
+// z transform of the columns i = 0..Nx/2 of a plane (cft with m = (Nx+2)/2).
+// With zero_row (SGN = +1) row Mz/2+1 is zeroed first, as four_to_phys_u
+// does (FOU3D.f90:668-670): each CTA reads its own columns of that row as
+// zero (its transform then overwrites them), and the first CTA of the plane
+// clears the slots beyond the transformed columns, which no CTA writes.
 template <int SGN>
-__device__ void plane_z(const Inst *__restrict__ insts, double *planes, int bc)
+__device__ void plane_z(const Inst *__restrict__ insts, double *planes, int bc, int zero_row)
 {
     extern __shared__ double2 sm[];
     const Inst &I = insts[0];
@@ -275,13 +279,12 @@ __device__ void plane_z(const Inst *__restrict__ insts, double *planes, int bc)
     const int ig2 = ig / 2;
     double2 *a = sm, *b = sm + Mz * bc;
     const int tot = Mz * bc;
-    if (SGN > 0) {  // zero row Mz/2+1 first (FOU3D.f90:668-670)
-        for (int t = threadIdx.x; t < ig2; t += blockDim.x) P[(size_t)(Mz / 2) * ig2 + t] = make_double2(0.0, 0.0);
-        __syncthreads();
-    }
+    const int zq = (SGN > 0 && zero_row) ? Mz / 2 : -1;
+    if (zq >= 0 && i0 == 0)
+        for (int t = nxh + threadIdx.x; t < ig2; t += blockDim.x) P[(size_t)zq * ig2 + t] = make_double2(0.0, 0.0);
     for (int t = threadIdx.x; t < tot; t += blockDim.x) {
         const int v = t % bc, q = t / bc, i = i0 + v;
-        a[q * bc + v] = i < nxh ? P[(size_t)q * ig2 + i] : make_double2(0.0, 0.0);
+        a[q * bc + v] = (i < nxh && q != zq) ? P[(size_t)q * ig2 + i] : make_double2(0.0, 0.0);
     }
     __syncthreads();
     double2 *r = fft_batch<SGN>(a, b, Mz, I.radz, I.nradz, bc, I.twz);
@@ -378,8 +381,11 @@ __device__ void plane_x(const Inst *__restrict__ insts, double *planes, int br)
     }
 }
 
-__global__ void k_plane_z_inv(const Inst *__restrict__ insts, double *planes, int bc) { plane_z<+1>(insts, planes, bc); }
-__global__ void k_plane_z_fwd(const Inst *__restrict__ insts, double *planes, int bc) { plane_z<-1>(insts, planes, bc); }
+__global__ void k_plane_z_inv(const Inst *__restrict__ insts, double *planes, int bc, int zero_row)
+{
+    plane_z<+1>(insts, planes, bc, zero_row);
+}
+__global__ void k_plane_z_fwd(const Inst *__restrict__ insts, double *planes, int bc) { plane_z<-1>(insts, planes, bc, 0); }
 __global__ void k_plane_x_inv(const Inst *__restrict__ insts, double *planes, int br) { plane_x<+1>(insts, planes, br); }
 __global__ void k_plane_x_fwd(const Inst *__restrict__ insts, double *planes, int br) { plane_x<-1>(insts, planes, br); }
 

@@ -49,6 +49,57 @@ static bool factor_fftpack(int n, const int try4[4], std::vector<int> &out)
     return true;
 }
 
+// Radix orders: cffti1 tries 3, 4, 2, 5 (cft_buff.f:144), rffti1 4, 2, 3
+// (rft_buff.f:136).
+bool cft_radices(int n, std::vector<int> &rad)
+{
+    static const int t[4] = {3, 4, 2, 5};
+    return factor_fftpack(n, t, rad);
+}
+
+bool rft_radices(int n, std::vector<int> &rad)
+{
+    static const int t[4] = {4, 2, 3, 5};
+    return factor_fftpack(n, t, rad);
+}
+
+// z twiddles with the rotation recurrence of cffti1 (cft_buff.f:166-179)
+void cft_table(int n, std::vector<double> &tw)
+{
+    tw.assign(2 * n, 0.0);
+    const double tpi = 8.0 * std::atan(1.0);
+    const double arg1 = tpi / (double)(float)n;
+    const double dc = std::cos(arg1), ds = std::sin(arg1);
+    std::vector<double> wa(2 * n);
+    wa[0] = dc;
+    wa[1] = ds;
+    for (int ii = 4; ii <= 2 * n; ii += 2) {
+        wa[ii - 2] = dc * wa[ii - 4] - ds * wa[ii - 3];
+        wa[ii - 1] = ds * wa[ii - 4] + dc * wa[ii - 3];
+    }
+    tw[0] = 1.0;
+    tw[1] = 0.0;
+    for (int t = 1; t < n; t++) {
+        tw[2 * t] = wa[2 * t - 2];
+        tw[2 * t + 1] = wa[2 * t - 1];
+    }
+}
+
+// x twiddles with direct cos/sin as rffti1 computes them
+void rft_table(int n, std::vector<double> &tw)
+{
+    tw.assign(2 * n, 0.0);
+    const double tpi = 2.0 * std::atan2(0.0, -1.0);
+    const double argh = tpi / (double)(float)n;
+    for (int t = 0; t < n; t++) {
+        const double arg = (double)t * argh;
+        tw[2 * t] = std::cos(arg);
+        tw[2 * t + 1] = std::sin(arg);
+    }
+    tw[0] = 1.0;
+    tw[1] = 0.0;
+}
+
 double flowrate_host(const HostSetup &s, const double *u1col)
 {
     double Qu = 0.0;
@@ -76,12 +127,11 @@ std::string build_setup(const lh_grid_desc &d, HostSetup &s)
     s.nc = s.nxh * d.Nz;
     s.nyv = d.ny - 2;
     s.nyu = s.nyv + 1;
-    static const int tz[4] = {3, 4, 2, 5}, tx[4] = {4, 2, 3, 5};
-    if (!factor_fftpack(s.Mz, tz, s.radz)) {
+    if (!cft_radices(s.Mz, s.radz)) {
         err << "Ngal_z = " << s.Mz << " is not 2/3-smooth";
         return err.str();
     }
-    if (!factor_fftpack(s.Mx, tx, s.radx) || s.Mx % 2) {
+    if (!rft_radices(s.Mx, s.radx) || s.Mx % 2) {
         err << "Ngal_x = " << s.Mx << " is not 2/3-smooth (rft_buff.f:308-311)";
         return err.str();
     }
@@ -260,39 +310,8 @@ std::string build_setup(const lh_grid_desc &d, HostSetup &s)
         factor_columns(0, nc);
     }
 
-    // ---- twiddles: z with the rotation recurrence of cffti1
-    // (cft_buff.f:166-179), x with direct cos/sin as rffti1 does
-    s.twz.assign(2 * s.Mz, 0.0);
-    {
-        const double tpi = 8.0 * std::atan(1.0);
-        const double arg1 = tpi / (double)(float)s.Mz;
-        const double dc = std::cos(arg1), ds = std::sin(arg1);
-        std::vector<double> wa(2 * s.Mz);
-        wa[0] = dc;
-        wa[1] = ds;
-        for (int ii = 4; ii <= 2 * s.Mz; ii += 2) {
-            wa[ii - 2] = dc * wa[ii - 4] - ds * wa[ii - 3];
-            wa[ii - 1] = ds * wa[ii - 4] + dc * wa[ii - 3];
-        }
-        s.twz[0] = 1.0;
-        s.twz[1] = 0.0;
-        for (int t = 1; t < s.Mz; t++) {
-            s.twz[2 * t] = wa[2 * t - 2];
-            s.twz[2 * t + 1] = wa[2 * t - 1];
-        }
-    }
-    s.twx.assign(2 * s.Mx, 0.0);
-    {
-        const double tpi = 2.0 * std::atan2(0.0, -1.0);
-        const double argh = tpi / (double)(float)s.Mx;
-        for (int t = 0; t < s.Mx; t++) {
-            const double arg = (double)t * argh;
-            s.twx[2 * t] = std::cos(arg);
-            s.twx[2 * t + 1] = std::sin(arg);
-        }
-        s.twx[0] = 1.0;
-        s.twx[1] = 0.0;
-    }
+    cft_table(s.Mz, s.twz);
+    rft_table(s.Mx, s.twx);
     return std::string();
 }
 

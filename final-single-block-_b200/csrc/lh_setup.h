@@ -27,6 +27,15 @@ struct HostSetup {
 // on success or the reason for rejection.
 std::string build_setup(const lh_grid_desc &d, HostSetup &s);
 
+// Radix plans (FFTPACK's factor orders, radices 2, 3, 4 only) and twiddle
+// tables exp(+2 pi i t / n), t < n, of the device transforms: complex z
+// transforms as cft, real x transforms as rft.  false when n has another
+// prime factor.
+bool cft_radices(int n, std::vector<int> &rad);
+bool rft_radices(int n, std::vector<int> &rad);
+void cft_table(int n, std::vector<double> &tw);
+void rft_table(int n, std::vector<double> &tw);
+
 // Flow rate of the (0,0) mode of a column-layout u1 (flowrateIm,
 // littleharsh.f90:473-492).
 double flowrate_host(const HostSetup &s, const double *u1col);

@@ -93,6 +93,16 @@ module lh_gpu_bridge
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
     end function
+    integer(c_int) function lh_pressure_snapshot(ctx) bind(C, name="lh_pressure_snapshot")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function lh_omega_x(ctx, out, cap) bind(C, name="lh_omega_x")
+      import :: c_int, c_ptr, c_double, c_size_t
+      type(c_ptr), value       :: ctx
+      real(c_double)           :: out(*)
+      integer(c_size_t), value :: cap
+    end function
     integer(c_int) function lh_get_stats(ctx, out, cap, count) bind(C, name="lh_get_stats")
       import :: c_int, c_ptr, c_double, c_size_t
       type(c_ptr), value       :: ctx
@@ -198,19 +208,33 @@ contains
     n = lh_get_spectra(gpu_ctx, 4_c_int, spP_, huge(0_c_size_t), n)
   end subroutine
 
-  ! stats(myid,status,ierr) where flagst and flagwr are both set (FOU3D.f90:340)
+  ! stats(myid,status,ierr) at the flagst steps (FOU3D.f90:307-341), with
+  ! omega_x formed on the device
   subroutine gpu_stats()
     call gpu_check(lh_stats_accumulate(gpu_ctx), 'lh_stats_accumulate')
   end subroutine
 
-  ! The nine plane sums acc(0:nyu+1, 9) = Um U2m Vm V2m Wm W2m UVm UWm VWm,
-  ! with the number of accumulations (istat)
+  ! ppPL = 0; modes_to_planes_UVP(ppPL, p, ...) on output steps (FOU3D.f90:149-152)
+  subroutine gpu_pressure_planes()
+    call gpu_check(lh_pressure_snapshot(gpu_ctx), 'lh_pressure_snapshot')
+  end subroutine
+
+  ! The plane sums acc(0:nyu+1, 13) = Um U2m Vm V2m Wm W2m UVm UWm VWm Pm P2m
+  ! wxm wx2m, with the number of accumulations (istat)
   subroutine gpu_fetch_stats(acc, nstat_done)
     real(8) :: acc(*)
     integer :: nstat_done
     integer(c_int) :: n, cnt
     n = lh_get_stats(gpu_ctx, acc, huge(0_c_size_t), cnt)
     nstat_done = cnt
+  end subroutine
+
+  ! omega_x at the v faces, wx(Nspec_x+2, Nspec_z, 0:nyu+1) in physical space
+  subroutine gpu_omega_x(wx)
+    real(8) :: wx(*)
+    integer(c_int) :: n
+    n = lh_omega_x(gpu_ctx, wx, huge(0_c_size_t))
+    if (n < 0) call gpu_check(n, 'lh_omega_x')
   end subroutine
 
   subroutine gpu_finalize()

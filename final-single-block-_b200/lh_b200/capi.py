@@ -30,7 +30,7 @@ EXPORTS = [
     "lh_instance_bytes", "lh_batch_add", "lh_batch_remove", "lh_batch_step",
     "lh_batch_download", "lh_batch_scalars", "lh_batch_count", "lh_batch_synchronize",
     "lh_spectra_accumulate", "lh_spectra_reset", "lh_get_spectra",
-    "lh_stats_accumulate", "lh_stats_reset", "lh_get_stats",
+    "lh_stats_accumulate", "lh_stats_reset", "lh_get_stats", "lh_pressure_snapshot", "lh_omega_x",
 ]
 
 
@@ -149,6 +149,8 @@ def lib() -> ctypes.CDLL:
         "lh_stats_accumulate": (i, [v]),
         "lh_stats_reset": (i, [v]),
         "lh_get_stats": (i, [v, dp, sz, P(i)]),
+        "lh_pressure_snapshot": (i, [v]),
+        "lh_omega_x": (i, [v, dp, sz]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -280,8 +282,8 @@ class Engine:
             out[name] = a.reshape(self.sizes.ncols, n // self.sizes.ncols)
         return out, cnt.value
 
-    # ---- stats of flagged output steps (stats.f90) ----------------------
-    STATS = ("Um", "U2m", "Vm", "V2m", "Wm", "W2m", "UVm", "UWm", "VWm")
+    # ---- stats of flagged steps (stats.f90) ------------------------------
+    STATS = ("Um", "U2m", "Vm", "V2m", "Wm", "W2m", "UVm", "UWm", "VWm", "Pm", "P2m", "wxm", "wx2m")
 
     def stats_accumulate(self):
         self._ck(self.L.lh_stats_accumulate(self.h), "stats_accumulate")
@@ -289,14 +291,31 @@ class Engine:
     def stats_reset(self):
         self._ck(self.L.lh_stats_reset(self.h), "stats_reset")
 
+    def pressure_snapshot(self):
+        """ppPL <- p, as nonlinear() does at output steps (FOU3D.f90:149-152)."""
+        self._ck(self.L.lh_pressure_snapshot(self.h), "pressure_snapshot")
+
     def stats(self) -> tuple[np.ndarray, int]:
-        """The nine plane sums as array[9, nyu+2] and the accumulation count."""
+        """The plane sums as array[13, nyu+2] (rows named by STATS) and the
+        accumulation count."""
         n = self.L.lh_get_stats(self.h, None, 0, None)
         if n < 0:
             self._ck(n, "stats")
         a, cnt = np.zeros(n), ctypes.c_int()
         self._ck(min(0, self.L.lh_get_stats(self.h, _dp(a), n, ctypes.byref(cnt))), "stats")
-        return a.reshape(9, n // 9), cnt.value
+        q = len(self.STATS)
+        return a.reshape(q, n // q), cnt.value
+
+    def omega_x(self) -> np.ndarray:
+        """omega_x of the current state (FOU3D.f90:314-338): [nyu+2, Nz, Nx+2],
+        physical values in [:, :, :Nx]."""
+        n = self.L.lh_omega_x(self.h, None, 0)
+        if n < 0:
+            self._ck(n, "omega_x")
+        a = np.zeros(n)
+        self._ck(min(0, self.L.lh_omega_x(self.h, _dp(a), n)), "omega_x")
+        sz = self.sizes
+        return a.reshape(sz.nyu + 2, sz.Nz, sz.Nx + 2)
 
     def stream(self) -> int:
         s = ctypes.c_void_p()

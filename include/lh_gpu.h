@@ -132,19 +132,36 @@ int lh_spectra_accumulate(lh_ctx *ctx);
 int lh_spectra_reset(lh_ctx *ctx);
 int lh_get_spectra(lh_ctx *ctx, int which, double *out, size_t cap, int *count);
 
-/* ---- stats of flagged output steps: replace stats() (stats.f90:1-97),
- * called from nonlinear() when both the stats and the output flags are set
- * (FOU3D.f90:300-341).  At that point the reference's plane arrays hold the
- * spectral coefficients placed by modes_to_planes_UVP, so its "plane sums"
- * run over those: lh_stats_accumulate adds, per plane j = 0..nyu+1, the nine
- * sums Um, U2m, Vm, V2m, Wm, W2m, UVm (u1 x u2 interpolated to the u rows),
- * UWm, VWm (u2 x u3 interpolated to the v rows) in the reference's order.
- * lh_get_stats copies out acc[9][nyu+2] and the count of accumulations.
- * Not built: Pm/P2m (the reference reads ppPL before refreshing it, i.e. the
- * pressure of the previous output step) and wxm/wx2m (omega_x). */
+/* ---- stats of flagged steps: replace stats() (stats.f90:1-97), which
+ * nonlinear() calls every nstat steps at kRK = 1 (FOU3D.f90:76-81, 290,
+ * 307-341), after ops_in_planes2 (FOU3D.f90:240) has transformed planes
+ * 1..nyu of its plane arrays to physical space in place (FOU3D.f90:1541,
+ * 1584).  lh_stats_accumulate adds into acc[13][nyu+2], j = 0..nyu+1:
+ *   0 Um 1 U2m  2 Vm 3 V2m  4 Wm 5 W2m  6 UVm (u1 x u2 interpolated to the
+ *   u rows)  7 UWm  8 VWm (u2 x u3 interpolated to the v rows) -- sums over
+ *   the physical Mx x Mz grid on planes 1..nyu, over the spectral
+ *   coefficients (re and im entries) on the wall planes 0 and nyu+1;
+ *   9 Pm 10 P2m -- over the spectral coefficients of the pressure planes of
+ *   the latest lh_pressure_snapshot (zero before the first), planes 1..nyu;
+ *   11 wxm 12 wx2m -- over omega_x = -d(u2)/dz + d(u3)/dy at the v faces in
+ *   physical space on the Nx x Nz grid (FOU3D.f90:314-338), planes 0..nyu+1.
+ * The physical-grid sums are evaluated from the spectral coefficients by
+ * Parseval's identity on the transform grid (the same sums; no transform
+ * runs).  lh_get_stats copies out acc and the count of accumulations. */
 int lh_stats_accumulate(lh_ctx *ctx);
 int lh_stats_reset(lh_ctx *ctx);
 int lh_get_stats(lh_ctx *ctx, double *out, size_t cap, int *count);
+/* ppPL <- p: nonlinear() refills the pressure planes at every output step
+ * (FOU3D.f90:149-152) and stats() reads them (stats.f90:45-52); call it
+ * where the reference's output flag is set, before that step's stats. */
+int lh_pressure_snapshot(lh_ctx *ctx);
+/* omega_x of the current state as nonlinear() forms it for stats()
+ * (modes_to_planes_phys, der_z_N, der_yv_h_wx, four_to_phys_N; FOU3D.f90:
+ * 314-338): (nyu+2) planes j = 0..nyu+1 of (Nx+2) x Nz doubles, x fastest,
+ * physical values in x = 1..Nx, host pointer.  Returns the element count;
+ * out = NULL only queries it.  The first call allocates a transform scratch
+ * of at most 256 MB. */
+int lh_omega_x(lh_ctx *ctx, double *out, size_t cap);
 
 /* ---- nonlinear-term intermediates of the last substep (parity) -------- */
 /* which: 0 Nu1 x/z part, 1 Nu2 x/z part, 2 Nu3 x/z part (FOU3D.f90:259-261

@@ -45,6 +45,9 @@ struct lho_ctx {
     double *DG;
     lho_cfft cz;
     lho_rfft rx;
+    lho_cfft czN; /* buffC_z: cft of length Nspec_z (start.f90:414-421) */
+    lho_rfft rxN; /* buffR_x: rft of length Nspec_x */
+    double *pp;   /* p as ppPL last held it (FOU3D.f90:151-152), column layout */
     /* column fields (re,im pairs) */
     double *u1, *u2, *u3, *p, *psi, *div;
     double *Nu1, *Nu2, *Nu3, *du1, *du2, *du3;
@@ -293,7 +296,8 @@ lho_ctx *lho_create(const lho_params *p)
 #ifdef _OPENMP
     c->nthr = p->nthreads > 0 ? p->nthreads : omp_get_max_threads();
 #endif
-    if (lho_cfft_init(&c->cz, c->Mz) != 0 || lho_rfft_init(&c->rx, c->Mx) != 0) {
+    if (lho_cfft_init(&c->cz, c->Mz) != 0 || lho_rfft_init(&c->rx, c->Mx) != 0 ||
+        lho_cfft_init(&c->czN, c->Nz) != 0 || lho_rfft_init(&c->rxN, c->Nx) != 0) {
         free(c);
         return NULL;
     }
@@ -396,7 +400,7 @@ void lho_destroy(lho_ctx *c)
                        &c->sav_nxz[0], &c->sav_nxz[1], &c->sav_nxz[2], &c->u1PL, &c->u2PL, &c->u3PL,
                        &c->u1PL_itp, &c->u2PL_itp, &c->u3PL_itp, &c->Nu1PL, &c->Nu2PL, &c->Nu3PL,
                        &c->uu_cPL, &c->uw_cPL, &c->vv_cPL, &c->ww_cPL, &c->uv_fPL, &c->wv_fPL,
-                       &c->a_ugrid, &c->a_vgrid, &c->u11};
+                       &c->a_ugrid, &c->a_vgrid, &c->u11, &c->pp};
     for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++) free(*bufs[i]);
     free(c->col_i);
     free(c->col_k);
@@ -1280,19 +1284,79 @@ void lho_spectra(lho_ctx *c, double *spU, double *spV, double *spW, double *spUV
     free(itp);
 }
 
-/* stats (stats.f90:1-97) at a flagged output step: the sums run over the
- * plane arrays as nonlinear() holds them when stats is called (FOU3D.f90:
- * 300-341), i.e. after modes_to_planes_UVP and before ops_in_planes2 -- the
- * spectral coefficients in the plane layout, entries i = 1..igal-2, rows
- * k = 1..kgal, planes limPL_incw (0..nyu+1 on every grid at one rank).
+/* The pressure planes stats() reads: nonlinear() refills ppPL from p at
+ * every output step (FOU3D.f90:149-152), and stats() runs only at kRK = 1
+ * (FOU3D.f90:290-341), so it sees p as of the latest output step. */
+void lho_pressure_snapshot(lho_ctx *c)
+{
+    const size_t n = 2 * (size_t)jlen(c, PGRID) * c->ncols;
+    if (!c->pp) c->pp = zalloc(n);
+    memcpy(c->pp, c->p, n * sizeof(double));
+}
+
+/* omega_x at the v faces as nonlinear() forms it before stats()
+ * (FOU3D.f90:314-338): u2 placed in Nspec-sized planes by
+ * modes_to_planes_phys (FOU3D.f90:816-860: dk_phys = 0, planes 0..nyv+1),
+ * der_z_N (FOU3D.f90:525-546, no masking), der_yv_h_wx (FOU3D.f90:592-610)
+ * placed the same way, -wx + du3dy over planes 0..nyu+1 (FOU3D.f90:331-336)
+ * and four_to_phys_N (FOU3D.f90:700-714: cft then rft of the Nspec sizes, no
+ * row zeroed).  Plane nyu+1, which the transposes never write, holds zeros.
+ * wx: (nyu+2) planes of (Nx+2) x Nz reals. */
+void lho_omega_x(lho_ctx *c, double *wx)
+{
+    const int Nx = c->Nx, Nz = c->Nz, ign = Nx + 2, nyv = c->nyv, nyu = c->nyu;
+    const int lu = jlen(c, UGRID), lv = jlen(c, VGRID);
+    const size_t plane = (size_t)ign * Nz;
+    const int nwork = 4 * (Nx > Nz ? Nx : Nz) + 8;
+#pragma omp parallel num_threads(c->nthr)
+    {
+        double *w = zalloc(nwork);
+#pragma omp for schedule(static)
+        for (int j = 0; j <= nyu + 1; j++) {
+            double *P = wx + plane * j;
+            memset(P, 0, plane * sizeof(double));
+            if (j <= nyv + 1) {
+                const double dth = c->dthdyv[j];
+                for (int col = 1; col <= c->ncols; col++) {
+                    const int i = c->col_i[col], k = c->col_k[col];
+                    const double *v = CX(c->u2, 0, lv, j, col);
+                    const double *a = CX(c->u3, 0, lu, j + 1, col), *b = CX(c->u3, 0, lu, j, col);
+                    double dz[2];
+                    mul_ik(c->k1z[k - 1], v, dz);
+                    const double dy0 = (a[0] - b[0]) * dth * c->ddthetavi;
+                    const double dy1 = (a[1] - b[1]) * dth * c->ddthetavi;
+                    P[2 * i + (size_t)ign * (k - 1)] = -dz[0] + dy0;
+                    P[2 * i + 1 + (size_t)ign * (k - 1)] = -dz[1] + dy1;
+                }
+            }
+            lho_cft(P, ign, 2, (Nx + 2) / 2, 1, &c->czN, w);
+            lho_rft(P, ign, Nz, 1, &c->rxN, w);
+        }
+        free(w);
+    }
+}
+
+/* stats (stats.f90:1-97) at a flagged output step.  nonlinear() calls it
+ * (FOU3D.f90:307-341) after ops_in_planes2 (FOU3D.f90:240), which has run
+ * four_to_phys_u in place on planes 1..nyu of u1PL, u2PL_itp, u3PL
+ * (FOU3D.f90:1541) and of u1PL_itp, u2PL, u3PL_itp (FOU3D.f90:1584; the v
+ * planes reach nyv+1 = nyu at one rank).  So on those planes the sums run over
+ * physical values, on the wall planes 0 and nyu+1 over the spectral
+ * coefficients modes_to_planes_UVP placed (zeros where it placed none):
+ * entries i = 1..igal-2, rows k = 1..kgal, planes limPL_incw (0..nyu+1 for u
+ * and v, 1..nyu+1 for p).  P sums read the pressure planes of the latest
+ * lho_pressure_snapshot (spectral, as modes_to_planes_UVP left them); wx sums
+ * run over the physical omega_x of lho_omega_x, i = 1..Nx, k = 1..Nz.
  * acc[q*(nyu+2) + j]: q 0 Um, 1 U2m, 2 Vm, 3 V2m, 4 Wm, 5 W2m, 6 UVm (u1 x
- * u2PL_itp), 7 UWm, 8 VWm (u2 x u3PL_itp). */
+ * u2PL_itp), 7 UWm, 8 VWm (u2 x u3PL_itp), 9 Pm, 10 P2m, 11 wxm, 12 wx2m. */
 void lho_stats(lho_ctx *c, double *acc)
 {
     const int nyu = c->nyu, nc = c->ncols, lu = jlen(c, UGRID), lv = jlen(c, VGRID);
-    const size_t plane = (size_t)c->igal * c->kgal, npl = (size_t)nyu + 2;
+    const int Nx = c->Nx, Nz = c->Nz, ign = Nx + 2;
+    const size_t plane = (size_t)c->igal * c->kgal, npl = (size_t)nyu + 2, planeN = (size_t)ign * Nz;
     double *P1 = zalloc(plane * npl), *P2 = zalloc(plane * npl), *P3 = zalloc(plane * npl);
-    double *P2i = zalloc(plane * npl), *P3i = zalloc(plane * npl);
+    double *P2i = zalloc(plane * npl), *P3i = zalloc(plane * npl), *PP = zalloc(plane * npl);
+    double *WX = zalloc(planeN * npl);
     double *u2i = zalloc(2 * (size_t)lu * nc), *u3i = zalloc(2 * (size_t)lv * nc);
     interp_v(c, u2i, c->u2);
     interp_u(c, u3i, c->u3);
@@ -1301,10 +1365,28 @@ void lho_stats(lho_ctx *c, double *acc)
     modes_to_planes(c, P3, c->u3, UGRID);
     modes_to_planes(c, P2i, u2i, UGRID);
     modes_to_planes(c, P3i, u3i, VGRID);
+    if (c->pp) modes_to_planes(c, PP, c->pp, PGRID);
+    lho_omega_x(c, WX);
+    const int nwork = 4 * (c->Mx > c->Mz ? c->Mx : c->Mz) + 8;
+#pragma omp parallel num_threads(c->nthr)
+    {
+        double *w = zalloc(nwork);
+#pragma omp for schedule(static)
+        for (int j = 1; j <= nyu; j++) {
+            four_to_phys_plane(c, PLANE(c, P1, j), w);
+            four_to_phys_plane(c, PLANE(c, P2i, j), w);
+            four_to_phys_plane(c, PLANE(c, P3, j), w);
+            four_to_phys_plane(c, PLANE(c, P2, j), w);
+            four_to_phys_plane(c, PLANE(c, P3i, j), w);
+        }
+        free(w);
+    }
+#pragma omp parallel for schedule(static) num_threads(c->nthr)
     for (int j = 0; j <= nyu + 1; j++) {
         double *Um = acc + 0 * npl + j, *U2m = acc + 1 * npl + j, *Vm = acc + 2 * npl + j, *V2m = acc + 3 * npl + j;
         double *Wm = acc + 4 * npl + j, *W2m = acc + 5 * npl + j, *UVm = acc + 6 * npl + j, *UWm = acc + 7 * npl + j;
-        double *VWm = acc + 8 * npl + j;
+        double *VWm = acc + 8 * npl + j, *Pm = acc + 9 * npl + j, *P2m = acc + 10 * npl + j;
+        double *wxm = acc + 11 * npl + j, *wx2m = acc + 12 * npl + j;
         for (int k = 1; k <= c->kgal; k++)
             for (int i = 1; i <= c->igal - 2; i++) {
                 const double a = *PL(c, P1, i, k, j), v = *PL(c, P2, i, k, j), w = *PL(c, P3, i, k, j);
@@ -1318,6 +1400,18 @@ void lho_stats(lho_ctx *c, double *acc)
                 *UVm = *UVm + a * vi;
                 *UWm = *UWm + a * w;
                 *VWm = *VWm + v * wi;
+                if (j >= 1) {
+                    const double q = *PL(c, PP, i, k, j);
+                    *Pm = *Pm + q;
+                    *P2m = *P2m + q * q;
+                }
+            }
+        const double *X = WX + planeN * j;
+        for (int k = 1; k <= Nz; k++)
+            for (int i = 1; i <= Nx; i++) {
+                const double x = X[(i - 1) + (size_t)ign * (k - 1)];
+                *wxm = *wxm + x;
+                *wx2m = *wx2m + x * x;
             }
     }
     free(P1);
@@ -1325,6 +1419,8 @@ void lho_stats(lho_ctx *c, double *acc)
     free(P3);
     free(P2i);
     free(P3i);
+    free(PP);
+    free(WX);
     free(u2i);
     free(u3i);
 }

@@ -130,10 +130,18 @@ double lho_error_div(const lho_ctx *c);
 void lho_spectra(lho_ctx *c, double *spU, double *spV, double *spW, double *spUV, double *spP);
 
 /* stats (stats.f90:1-97): add the plane sums of the current state into
- * acc[9][nyu+2] (Um U2m Vm V2m Wm W2m UVm UWm VWm over planes 0..nyu+1); the
- * planes hold the spectral coefficients in the plane layout, as they do in
- * nonlinear() when stats is called (FOU3D.f90:300-341). */
+ * acc[13][nyu+2] (Um U2m Vm V2m Wm W2m UVm UWm VWm over planes 0..nyu+1, in
+ * physical space on planes 1..nyu and over the spectral coefficients on the
+ * wall planes, as nonlinear() holds them when it calls stats (FOU3D.f90:
+ * 240, 307-341); Pm P2m over planes 1..nyu+1 of the latest pressure
+ * snapshot; wxm wx2m over the physical omega_x of lho_omega_x). */
 void lho_stats(lho_ctx *c, double *acc);
+/* ppPL <- p as nonlinear() does at output steps (FOU3D.f90:149-152); the
+ * snapshot is zero until the first call */
+void lho_pressure_snapshot(lho_ctx *c);
+/* omega_x of the current state at planes 0..nyu+1 (FOU3D.f90:314-338):
+ * (nyu+2) planes of (Nx+2) x Nz reals, physical values at i = 1..Nx */
+void lho_omega_x(lho_ctx *c, double *wx);
 
 /* generic mode-count helpers for the 2-D (i,k) <-> plane map */
 int lho_column_i(const lho_ctx *c, int column);   /* 1-based column */

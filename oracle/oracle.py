@@ -87,6 +87,8 @@ def lib(threaded: bool = False) -> ctypes.CDLL:
     L.lho_error_div.argtypes = [v]
     L.lho_spectra.argtypes = [v, dp, dp, dp, dp, dp]
     L.lho_stats.argtypes = [v, dp]
+    L.lho_pressure_snapshot.argtypes = [v]
+    L.lho_omega_x.argtypes = [v, dp]
     L.lho_cfft_init.restype = i
     L.lho_rfft_init.restype = i
     _libs[threaded] = L
@@ -195,14 +197,25 @@ class Oracle:
     def error_div(self) -> float:
         return self.L.lho_error_div(self.h)
 
-    STATS = ("Um", "U2m", "Vm", "V2m", "Wm", "W2m", "UVm", "UWm", "VWm")
+    STATS = ("Um", "U2m", "Vm", "V2m", "Wm", "W2m", "UVm", "UWm", "VWm", "Pm", "P2m", "wxm", "wx2m")
 
     def stats(self, acc: np.ndarray | None = None) -> np.ndarray:
-        """stats() at a flagged output step: add into acc[9, nyu+2] (new zeros when None)."""
+        """stats() at a flagged output step: add into acc[13, nyu+2] (new zeros when None)."""
         if acc is None:
-            acc = np.zeros((9, self.nyu + 2))
+            acc = np.zeros((len(self.STATS), self.nyu + 2))
         self.L.lho_stats(self.h, _dp(acc))
         return acc
+
+    def pressure_snapshot(self) -> None:
+        """ppPL <- p, as nonlinear() does at output steps (FOU3D.f90:149-152)."""
+        self.L.lho_pressure_snapshot(self.h)
+
+    def omega_x(self) -> np.ndarray:
+        """omega_x of the current state (FOU3D.f90:314-338): [nyu+2, Nz, Nx+2],
+        physical values in [:, :, :Nx]."""
+        wx = np.zeros((self.nyu + 2, self.Nz, self.Nx + 2))
+        self.L.lho_omega_x(self.h, _dp(wx))
+        return wx
 
     def spectra(self, acc: dict | None = None) -> dict:
         """spectra() at a flagged step: add the current state's terms into acc

@@ -10,6 +10,8 @@
   370-409) and the time step follows the CFL rule (FOU3D.f90:290-303).
 * The spectra of flagged steps (spectra.f90:7-66) against a direct statement
   of buildsp/buildspUV with interp_v.
+* The plane stats (stats.f90:1-97) and omega_x (FOU3D.f90:314-338) against a
+  numpy statement with numpy's FFT in the reference's conventions.
 """
 import os
 
@@ -125,23 +127,113 @@ def test_oracle_spectra_follow_spectra_f90():
         assert np.max(abs(acc[k] - r)) <= 1e-14 * np.max(abs(r)), k
 
 
+def _ngal_planes(o, x):
+    """columns [col, j] -> spectral planes [j, Mz, Nx/2+1] in the dealiased row
+    order of modes_to_planes_UVP (start.f90:1031-1040)."""
+    nxh = o.Nx // 2 + 1
+    X = x.T.reshape(x.shape[1], o.Nz, nxh)
+    P = np.zeros((x.shape[1], o.Mz, nxh), complex)
+    P[:, :o.Nz // 2] = X[:, :o.Nz // 2]
+    P[:, o.Mz - o.Nz // 2:] = X[:, o.Nz // 2:]
+    return P
+
+
+def _to_phys(P, M):
+    """cft backward (unscaled) along z, then rft backward along x, which
+    ignores the imaginary parts of modes 0 and M/2 (rft_buff.f:78-81)."""
+    c = np.fft.ifft(P, axis=1) * P.shape[1]
+    full = np.zeros(P.shape[:2] + (M // 2 + 1,), complex)
+    full[..., :P.shape[2]] = c
+    return np.fft.irfft(full, n=M, axis=2) * M
+
+
 def test_oracle_stats_follow_stats_f90():
-    """lho_stats sums, per plane, the spectral coefficients the plane arrays
-    hold when stats() runs (re and im entries): Um = sum(Re + Im), U2m =
-    sum |u1|^2, V2m = sum |u2|^2 over the v planes (zero above nyv+1)."""
+    """lho_stats against a numpy statement of stats() as nonlinear() calls it
+    (FOU3D.f90:240, 307-341): planes 1..nyu in physical space after
+    four_to_phys_u, wall planes over the spectral coefficients (Re + Im
+    entries), Pm/P2m over the pressure snapshot's coefficients, wxm/wx2m over
+    omega_x = -d(u2)/dz + d(u3)/dy at the faces in physical space of the
+    Nspec grid (FOU3D.f90:314-338)."""
     from lh_b200 import Desc, grids, perturbed_laminar
-    d = Desc(Nx=16, Nz=16, ny=33, dt_mode=1, dt=1e-3)
+    N, ny = 16, 33
+    d = Desc(Nx=N, Nz=N, ny=ny, dt_mode=1, dt=1e-3)
     yu, yv = grids(d)
-    o = O.Oracle(O.Config(Nx=16, Nz=16, ny=33, dt_mode=O.DT_FIXED, dt_fixed=1e-3))
+    o = O.Oracle(O.Config(Nx=N, Nz=N, ny=ny, dt_mode=O.DT_FIXED, dt_fixed=1e-3))
     o.load_state(*perturbed_laminar(d, 3, yu, yv))
+    o.step(1)
+    o.pressure_snapshot()
+    pp = o.state()["p"]
     o.step(1)
     acc = o.stats()
     st = o.state()
     u1, u2, u3 = st["u1"], st["u2"], st["u3"]
-    scale = np.max(abs(u1)) ** 2 * u1.shape[0]
-    assert np.max(abs(acc[0] - (u1.real + u1.imag).sum(0))) <= 1e-13 * scale
-    assert np.max(abs(acc[1] - (abs(u1) ** 2).sum(0))) <= 1e-13 * scale
-    v2 = np.zeros(d.nyu + 2)
-    v2[:d.nyv + 2] = (abs(u2) ** 2).sum(0)
-    assert np.max(abs(acc[3] - v2)) <= 1e-13 * scale
-    assert np.max(abs(acc[7] - (u1.real * u3.real + u1.imag * u3.imag).sum(0))) <= 1e-13 * scale
+    nyu, nyv, Mx, Mz = d.nyu, d.nyv, o.Mx, o.Mz
+    # interpolations (interp_v, interp_u; FOU3D.f90:373-418)
+    u2i = np.zeros_like(u1)
+    for j in range(1, nyu + 1):
+        u2i[:, j] = ((yu[j] - yv[j - 1]) * u2[:, j] + (yv[j] - yu[j]) * u2[:, j - 1]) / (yv[j] - yv[j - 1])
+    g1 = (yu[0] - yu[1]) / (yv[0] - yu[1])
+    g2 = (yu[nyu + 1] - yu[nyu]) / (yv[nyu] - yu[nyu])
+    u2i[:, 0] = g1 * (u2[:, 0] - u2i[:, 1]) + u2i[:, 1]
+    u2i[:, -1] = g2 * (u2[:, -1] - u2i[:, -2]) + u2i[:, -2]
+    u3i = np.zeros_like(u2)
+    for j in range(nyv + 2):
+        u3i[:, j] = ((yv[j] - yu[j]) * u3[:, j + 1] + (yu[j + 1] - yv[j]) * u3[:, j]) / (yu[j + 1] - yu[j])
+    pad = lambda a: np.concatenate([a, np.zeros((a.shape[0], nyu + 2 - a.shape[1]), complex)], axis=1)
+    F = {k: _ngal_planes(o, v) for k, v in
+         (("a", u1), ("w", u3), ("vi", u2i), ("v", pad(u2)), ("wi", pad(u3i)))}
+    ph = {k: _to_phys(v[1:nyu + 1], Mx) for k, v in F.items()}
+    ref = np.zeros((13, nyu + 2))
+    lin = lambda z: (z.real + z.imag).sum()
+    dot = lambda x, y: (x.real * y.real + x.imag * y.imag).sum()
+    for j in (0, nyu + 1):   # wall planes keep their spectral coefficients
+        a, w, vi, v, wi = (F[k][j] for k in ("a", "w", "vi", "v", "wi"))
+        ref[:9, j] = [lin(a), dot(a, a), lin(v), dot(v, v), lin(w), dot(w, w), dot(a, vi), dot(a, w), dot(v, wi)]
+    a, w, vi, v, wi = (ph[k] for k in ("a", "w", "vi", "v", "wi"))
+    S = lambda x: x.sum(axis=(1, 2))
+    ref[:9, 1:nyu + 1] = [S(a), S(a * a), S(v), S(v * v), S(w), S(w * w), S(a * vi), S(a * w), S(v * wi)]
+    for j in range(1, nyu + 1):
+        ref[9, j], ref[10, j] = lin(pp[:, j - 1]), dot(pp[:, j - 1], pp[:, j - 1])
+    # omega_x spectral (der_z_N, der_yv_h_wx), then four_to_phys_N on the Nspec grid
+    dthdyv = o.array(3)
+    kz = d.bet * np.repeat(np.where(np.arange(N) < N // 2, np.arange(N), np.arange(N) - N), N // 2 + 1)
+    wxh = np.zeros((u1.shape[0], nyu + 2), complex)
+    for j in range(nyv + 2):
+        wxh[:, j] = -(1j * kz * u2[:, j]) + (u3[:, j + 1] - u3[:, j]) * dthdyv[j]
+    wxp = _to_phys(wxh.T.reshape(nyu + 2, N, N // 2 + 1), N)
+    ref[11], ref[12] = S(wxp), S(wxp * wxp)
+    fmax = max(np.max(abs(x)) for x in ph.values())
+    n = Mx * Mz
+    for q, name in enumerate(O.Oracle.STATS):
+        if name.startswith("wx"):
+            scale = N * N * np.max(abs(wxp)) ** (2 if name == "wx2m" else 1)
+        else:
+            scale = n * fmax ** (1 if name in ("Um", "Vm", "Wm", "Pm") else 2)
+        assert np.max(abs(acc[q] - ref[q])) <= 1e-13 * scale, (name, np.max(abs(acc[q] - ref[q])), scale)
+    # the wall planes and the pressure rows are plain sums of coefficients
+    assert np.allclose(acc[9:11], ref[9:11], rtol=1e-13, atol=0)
+    assert acc[9, 0] == 0.0 and acc[9, nyu + 1] == 0.0
+
+
+def test_oracle_omega_x_is_the_curl_on_the_nspec_grid():
+    """lho_omega_x equals the x vorticity of the state evaluated by numpy on
+    the Nx x Nz grid: -d(u2)/dz from the spectral derivative and
+    d(u3)/dy from the face difference, planes 0..nyv+1, zero above."""
+    from lh_b200 import Desc, grids, perturbed_laminar
+    N, ny = 16, 33
+    d = Desc(Nx=N, Nz=N, ny=ny, dt_mode=1, dt=1e-3)
+    yu, yv = grids(d)
+    o = O.Oracle(O.Config(Nx=N, Nz=N, ny=ny, dt_mode=O.DT_FIXED, dt_fixed=1e-3))
+    o.load_state(*perturbed_laminar(d, 5, yu, yv))
+    wx = o.omega_x()
+    st = o.state()
+    u2, u3 = st["u2"], st["u3"]
+    dthdyv = o.array(3)
+    kz = d.bet * np.repeat(np.where(np.arange(N) < N // 2, np.arange(N), np.arange(N) - N), N // 2 + 1)
+    wxh = np.zeros((u2.shape[0], d.nyu + 2), complex)
+    for j in range(d.nyv + 2):
+        wxh[:, j] = -(1j * kz * u2[:, j]) + (u3[:, j + 1] - u3[:, j]) * dthdyv[j]
+    ref = _to_phys(wxh.T.reshape(d.nyu + 2, N, N // 2 + 1), N)
+    assert wx.shape == (d.nyu + 2, N, N + 2)
+    assert np.max(abs(wx[:, :, :N] - ref)) <= 1e-13 * np.max(abs(ref))
+    assert not np.any(wx[d.nyu + 1])
