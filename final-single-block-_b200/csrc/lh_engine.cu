@@ -288,26 +288,27 @@ ClassTiles fast_tiles(const HostSetup &s, int cbz_max, int rb, int cbf_max)
     c.fast = true;
     const size_t smax = 110 * 1024;
     auto fits = [&](int stage, int M, int vectors, int per) {
-        return fast_threads(M, vectors) <= fast_max_threads(stage) && (size_t)M * (1 + per) * 16 <= smax;
+        return fast_threads(M, vectors) <= fast_max_threads(stage) && (size_t)M * per * 16 <= smax;
     };
     cbz_max = std::max(1, std::min(cbz_max, s.nxh));
     while (cbz_max > 1 && !fits(0, s.Mz, cbz_max, cbz_max)) cbz_max--;
     int nb = (s.nxh + cbz_max - 1) / cbz_max;
     c.cbz = (s.nxh + nb - 1) / nb;
     c.tz = fast_threads(s.Mz, c.cbz);
-    c.smz = (size_t)s.Mz * (1 + c.cbz) * sizeof(double2);
+    c.smz = (size_t)s.Mz * c.cbz * sizeof(double2);
     rb = std::max(1, std::min(rb, s.Mz));
-    while (rb > 1 && !fits(1, s.Mx, 3 * rb, 3 * rb)) rb--;
+    // the x stage's vectors sit at an odd row stride (3 rb rounded up to odd)
+    while (rb > 1 && !fits(1, s.Mx, 3 * rb, (3 * rb) | 1)) rb--;
     c.rbx = rb;
     c.tx = fast_threads(s.Mx, 3 * rb);
-    c.smx = (size_t)s.Mx * (1 + 3 * rb) * sizeof(double2);
+    c.smx = (size_t)s.Mx * ((3 * rb) | 1) * sizeof(double2);
     cbf_max = std::max(1, std::min(cbf_max, s.nxh));
     // z forward: one half of the six products (3 vectors per x mode) per CTA
-    while (cbf_max > 1 && !fits(2, s.Mz, 3 * cbf_max, 3 * cbf_max)) cbf_max--;
+    while (cbf_max > 1 && !fits(2, s.Mz, 3 * cbf_max, (3 * cbf_max) | 1)) cbf_max--;
     nb = (s.nxh + cbf_max - 1) / cbf_max;
     c.cbf = (s.nxh + nb - 1) / nb;
     c.tf = fast_threads(s.Mz, 3 * c.cbf);
-    c.smf = (size_t)s.Mz * (1 + 3 * c.cbf) * sizeof(double2);
+    c.smf = (size_t)s.Mz * ((3 * c.cbf) | 1) * sizeof(double2);
     return c;
 }
 

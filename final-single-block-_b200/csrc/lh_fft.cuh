@@ -4,8 +4,9 @@
 // (natural order in and out) by mixed-radix Cooley-Tukey splits R = P*Q,
 // P in {4, 3, 2}; all indices are compile-time constants and the internal
 // twiddles are immediates (RootSel).  The outer twiddles of the two-pass
-// long transform come from a table tw[m] = exp(+2 pi i m / NT) in shared
-// memory (the rotation-recurrence table for z, direct cos/sin for x).
+// long transform start from one entry per lane of the table
+// tw[m] = exp(+2 pi i m / NT) in global memory (the rotation-recurrence
+// table for z, direct cos/sin for x).
 //
 // A length-N transform of a batch is done in two passes, N = N1 * N2:
 //   pass 1: per (vector, n2): DFT_N1 over x[n2 + N2 n1], twiddle W_N^(n2 k1)
@@ -208,10 +209,5 @@ struct FastDiv {
 
 // Sizes with a compiled fast path (Ngal = 3N/2 of the usual channel grids).
 #define LH_FAST_SIZES(X) X(12) X(24) X(48) X(96) X(144) X(192) X(288) X(384)
-
-__device__ __forceinline__ void load_table(double2 *dst, const double2 *__restrict__ src, int n)
-{
-    for (int t = threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
-}
 
 }  // namespace lh

@@ -2,8 +2,9 @@
 //
 // Every transform is a two-pass register FFT (lh_fft.cuh) whose index
 // arithmetic folds to constants; one template per stage, instantiated for
-// the Ngal sizes of the usual grids.  One CTA per work item; the twiddle
-// table is copied into shared memory per CTA.
+// the Ngal sizes of the usual grids.  One CTA per work item; each lane reads
+// its one outer-twiddle base from the table in global memory, so shared
+// memory holds only the transform data.
 //
 // Staging (per instance, inside I.S; the kRoundStreams chunk rounds in
 // flight use disjoint shares):
@@ -50,7 +51,7 @@ namespace lh {
 // unit); the recurrence's rounding stays within a few ulp for k1 <= 24.
 struct TwStep {
     double2 w1, wk;
-    __device__ explicit TwStep(const double2 *tw, int r) : w1(tw[r]), wk(make_double2(1.0, 0.0)) {}
+    __device__ explicit TwStep(double2 base) : w1(base), wk(make_double2(1.0, 0.0)) {}
     __device__ __forceinline__ double2 next()
     {
         wk = make_double2(wk.x * w1.x - wk.y * w1.y, wk.x * w1.y + wk.y * w1.x);
@@ -77,10 +78,11 @@ __global__ void __launch_bounds__(LH_ZINV_T, LH_ZINV_B) k_zinv_f(const Inst *__r
     constexpr int N1 = Plan2<NZ>::N1, N2 = Plan2<NZ>::N2;
     constexpr int Nz = 2 * NZ / 3;
     extern __shared__ double2 sm[];
-    double2 *tw = sm, *T = sm + NZ;
+    double2 *T = sm;
     if ((int)blockIdx.x >= count) return;
-    load_table(tw, insts[work[blockIdx.x].inst].twz, NZ);  // depends on Mz only
+    const double2 *tw = insts[work[blockIdx.x].inst].twz;  // depends on Mz only
     const int t = threadIdx.x, v = t % cb, r = t / cb;
+    const double2 twr = __ldg(tw + r);  // outer-twiddle base W^r, issued before the data loads
     {
         const Work w = work[blockIdx.x];
         const Inst &I = insts[w.inst];
@@ -89,7 +91,6 @@ __global__ void __launch_bounds__(LH_ZINV_T, LH_ZINV_B) k_zinv_f(const Inst *__r
         const int f = w.blk / nblk, i = (w.blk % nblk) * cb + v;
         const double2 *src = (f == 0 ? I.U1 : (f == 1 ? I.U3 : I.U2)) + (size_t)w.j * nc;
         const bool ok = i < nxh;
-        __syncthreads();  // table loaded / T free
         if (r < N2) {
             double2 a[N1];
 #pragma unroll
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(LH_ZINV_T, LH_ZINV_B) k_zinv_f(const Inst *__r
                 a[n1] = (kr >= 0 && ok) ? src[kr * nxh + i] : make_double2(0.0, 0.0);
             }
             DFT<N1, +1, NZ>::run(a, tw);
-            TwStep ts(tw, r);
+            TwStep ts(twr);
 #pragma unroll
             for (int k1 = 0; k1 < N1; k1++) {
                 double2 z = a[k1];
@@ -138,10 +139,13 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
     constexpr int N1 = Plan2<NX>::N1, N2 = Plan2<NX>::N2;
     extern __shared__ double2 sm[];
     __shared__ double red[2][16];
-    double2 *tw = sm, *buf = sm + NX;
+    double2 *buf = sm;
     if ((int)blockIdx.x >= count) return;
-    load_table(tw, insts[work[blockIdx.x].inst].twx, NX);  // depends on Mx only
-    const int t = threadIdx.x, nv = 3 * rb, v = t % nv, r = t / nv;
+    const double2 *tw = insts[work[blockIdx.x].inst].twx;  // depends on Mx only
+    // buf[x][v] with an odd row stride ld (double2): the column-wise gather
+    // and pass-2 accesses then spread over all bank groups
+    const int t = threadIdx.x, nv = 3 * rb, ld = nv | 1, v = t % nv, r = t / nv;
+    const double2 twr = __ldg(tw + r);  // outer-twiddle base W^r, issued before the data loads
     constexpr int nxh = NX / 3 + 1;  // Nx/2 + 1 with Mx = 3 Nx / 2
     const FastDiv by_rb(rb), by_nv(nv);
     {
@@ -157,7 +161,6 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
         const double w0v = (I.yu[j] - I.yv[j - 1]) * dnv, w1v = (I.yv[j] - I.yu[j]) * dnv;
         const double w0u = (I.yv[j] - I.yu[j]) * dnu, w1u = (I.yu[j + 1] - I.yv[j]) * dnu;
         double2 *S = sprod_slot(I, w.slot);
-        __syncthreads();  // table loaded / buf free
         // (0) coalesced gather of the rows (k fastest) straight into the packed
         // complex vectors of the inverse transform, z[n][v] (v = pair*rb + row):
         // z = A + iB for the two real rows A, B of a pair, Hermitian-extended,
@@ -186,28 +189,31 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
             if (k == 0) {
                 buf[vv] = make_double2(A.x, B.x);
             } else {
-                buf[k * nv + vv] = make_double2(A.x - B.y, A.y + B.x);
-                buf[(NX - k) * nv + vv] = make_double2(A.x + B.y, B.x - A.y);
+                buf[k * ld + vv] = make_double2(A.x - B.y, A.y + B.x);
+                buf[(NX - k) * ld + vv] = make_double2(A.x + B.y, B.x - A.y);
             }
         }
-        for (int e = t; e < (NX - 2 * nxh + 1) * nv; e += blockDim.x) buf[nxh * nv + e] = make_double2(0.0, 0.0);
+        for (int e = t; e < (NX - 2 * nxh + 1) * nv; e += blockDim.x) {
+            const int x = by_nv.div(e);
+            buf[(nxh + x) * ld + by_nv.mod(e, x)] = make_double2(0.0, 0.0);
+        }
         __syncthreads();
         // (1) inverse pass 1: lane r < N2 holds n = r + N2*n1
         {
             double2 a[N1];
             if (r < N2) {
 #pragma unroll
-                for (int n1 = 0; n1 < N1; n1++) a[n1] = buf[(r + N2 * n1) * nv + v];
+                for (int n1 = 0; n1 < N1; n1++) a[n1] = buf[(r + N2 * n1) * ld + v];
             }
             __syncthreads();
             if (r < N2) {
                 DFT<N1, +1, NX>::run(a, tw);
-                TwStep ts(tw, r);
+                TwStep ts(twr);
 #pragma unroll
                 for (int k1 = 0; k1 < N1; k1++) {
                     double2 z = a[k1];
                     if (k1 > 0) z = twiddle<+1>(ts.next(), z);
-                    buf[(k1 * N2 + r) * nv + v] = z;
+                    buf[(k1 * N2 + r) * ld + v] = z;
                 }
             }
         }
@@ -217,13 +223,13 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
             double2 b[N2];
             if (r < N1) {
 #pragma unroll
-                for (int n2 = 0; n2 < N2; n2++) b[n2] = buf[(r * N2 + n2) * nv + v];
+                for (int n2 = 0; n2 < N2; n2++) b[n2] = buf[(r * N2 + n2) * ld + v];
                 DFT<N2, +1, NX>::run(b, tw);
             }
             __syncthreads();
             if (r < N1) {
 #pragma unroll
-                for (int k2 = 0; k2 < N2; k2++) buf[(r + N1 * k2) * nv + v] = b[k2];
+                for (int k2 = 0; k2 < N2; k2++) buf[(r + N1 * k2) * ld + v] = b[k2];
             }
         }
         __syncthreads();
@@ -233,7 +239,7 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
         double m1 = 0.0, m3 = 0.0;
         for (int e = t; e < NX * rb; e += blockDim.x) {
             const int x = by_rb.div(e), r2 = by_rb.mod(e, x);
-            double2 *p = buf + x * nv;
+            double2 *p = buf + x * ld;
             const double2 p0 = p[r2], p1 = p[rb + r2], p2 = p[2 * rb + r2];
             const double u1 = p0.x, u3 = p0.y, u2c = p1.x, u2 = p1.y, u1f = p2.x, u3f = p2.y;
             if (track && q0 + r2 < Mz) {
@@ -269,17 +275,17 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
             double2 a[N1];
             if (r < N2) {
 #pragma unroll
-                for (int n1 = 0; n1 < N1; n1++) a[n1] = buf[(r + N2 * n1) * nv + v];
+                for (int n1 = 0; n1 < N1; n1++) a[n1] = buf[(r + N2 * n1) * ld + v];
                 DFT<N1, -1, NX>::run(a, tw);
             }
             __syncthreads();
             if (r < N2) {
-                TwStep ts(tw, r);
+                TwStep ts(twr);
 #pragma unroll
                 for (int k1 = 0; k1 < N1; k1++) {
                     double2 z = a[k1];
                     if (k1 > 0) z = twiddle<-1>(ts.next(), z);
-                    buf[(k1 * N2 + r) * nv + v] = z;
+                    buf[(k1 * N2 + r) * ld + v] = z;
                 }
             }
         }
@@ -289,13 +295,13 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
             double2 b[N2];
             if (r < N1) {
 #pragma unroll
-                for (int n2 = 0; n2 < N2; n2++) b[n2] = buf[(r * N2 + n2) * nv + v];
+                for (int n2 = 0; n2 < N2; n2++) b[n2] = buf[(r * N2 + n2) * ld + v];
                 DFT<N2, -1, NX>::run(b, tw);
             }
             __syncthreads();
             if (r < N1) {
 #pragma unroll
-                for (int k2 = 0; k2 < N2; k2++) buf[(r + N1 * k2) * nv + v] = b[k2];
+                for (int k2 = 0; k2 < N2; k2++) buf[(r + N1 * k2) * ld + v] = b[k2];
             }
         }
         __syncthreads();
@@ -305,8 +311,8 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
             const int k = by_nv.div(e), vv = by_nv.mod(e, k);
             const int p2 = by_rb.div(vv), r2 = by_rb.mod(vv, p2), qq = q0 + r2;
             if (qq >= Mz) continue;
-            const double2 zk = buf[k * nv + vv];
-            const double2 zm = buf[(k == 0 ? 0 : NX - k) * nv + vv];
+            const double2 zk = buf[k * ld + vv];
+            const double2 zm = buf[(k == 0 ? 0 : NX - k) * ld + vv];
             double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
             double2 B = make_double2(0.5 * (zk.y + zm.y), 0.5 * (zm.x - zk.x));
             if (k == 0) {
@@ -332,10 +338,12 @@ __global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_f(const Inst *__r
     constexpr int N1 = Plan2<NZ>::N1, N2 = Plan2<NZ>::N2;
     constexpr int Nz = 2 * NZ / 3;
     extern __shared__ double2 sm[];
-    double2 *tw = sm, *T = sm + NZ;
+    double2 *T = sm;
     if ((int)blockIdx.x >= count) return;
-    load_table(tw, insts[work[blockIdx.x].inst].twz, NZ);  // depends on Mz only
-    const int t = threadIdx.x, nv = 3 * cb, v = t % nv, r = t / nv;
+    const double2 *tw = insts[work[blockIdx.x].inst].twz;  // depends on Mz only
+    // T[z][v] with an odd row stride ld (double2), as in the x stage
+    const int t = threadIdx.x, nv = 3 * cb, ld = nv | 1, v = t % nv, r = t / nv;
+    const double2 twr = __ldg(tw + r);  // outer-twiddle base W^r, issued before the data loads
     const int f = v / cb, c = v % cb;
     const FastDiv by_cb(cb);
     {
@@ -347,19 +355,18 @@ __global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_f(const Inst *__r
         const int g = h == 0 ? (f == 2 ? 3 : f) : (f == 0 ? 2 : f + 3);  // product of this vector
         const double2 *S = sprod_slot(I, w.slot);
         const bool ok = i < nxh;
-        __syncthreads();  // table loaded / T free
         if (r < N2) {
             double2 a[N1];
 #pragma unroll
             for (int n1 = 0; n1 < N1; n1++)
                 a[n1] = ok ? S[((size_t)g * NZ + r + N2 * n1) * nxh + i] : make_double2(0.0, 0.0);
             DFT<N1, -1, NZ>::run(a, tw);
-            TwStep ts(tw, r);
+            TwStep ts(twr);
 #pragma unroll
             for (int k1 = 0; k1 < N1; k1++) {
                 double2 z = a[k1];
                 if (k1 > 0) z = twiddle<-1>(ts.next(), z);
-                T[(k1 * N2 + r) * nv + v] = z;
+                T[(k1 * N2 + r) * ld + v] = z;
             }
         }
         __syncthreads();
@@ -367,14 +374,14 @@ __global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_f(const Inst *__r
             double2 b[N2];
             if (r < N1) {
 #pragma unroll
-                for (int n2 = 0; n2 < N2; n2++) b[n2] = T[(r * N2 + n2) * nv + v];
+                for (int n2 = 0; n2 < N2; n2++) b[n2] = T[(r * N2 + n2) * ld + v];
                 DFT<N2, -1, NZ>::run(b, tw);
             }
             __syncthreads();
             if (r < N1) {
                 const double dn1 = 1.0 / NZ;
 #pragma unroll
-                for (int k2 = 0; k2 < N2; k2++) T[(r + N1 * k2) * nv + v] = make_double2(dn1 * b[k2].x, dn1 * b[k2].y);
+                for (int k2 = 0; k2 < N2; k2++) T[(r + N1 * k2) * ld + v] = make_double2(dn1 * b[k2].x, dn1 * b[k2].y);
             }
         }
         __syncthreads();
@@ -382,7 +389,7 @@ __global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_f(const Inst *__r
             const int kr = by_cb.div(e), cc = by_cb.mod(e, kr), ii = i0 + cc;
             if (ii >= nxh) continue;
             const int zp = kr < Nz / 2 ? kr : kr + NZ - Nz;
-            const double2 *row = T + zp * nv + cc;
+            const double2 *row = T + zp * ld + cc;
             const double2 p0 = row[0], p1 = row[cb], p2 = row[2 * cb];
             const size_t on = (size_t)(j - 1) * nc + kr * nxh + ii;
             const bool keep = kr != Nz / 2;  // der_x/der_z zero the kz = -Nz/2 row (FOU3D.f90:444-447)
