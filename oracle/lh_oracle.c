@@ -1294,13 +1294,24 @@ void lho_pressure_snapshot(lho_ctx *c)
     memcpy(c->pp, c->p, n * sizeof(double));
 }
 
+/* der_z_N (FOU3D.f90:525-546): dudz(i,k) = kz(k) u(i,k) on the complex view
+ * (0:Nx/2, Nz) of an (Nx+2) x Nz real plane, every row, no masking; kz_im
+ * holds the imaginary parts of kz(1:Nz) */
+void lho_der_z_n(const double *u, double *dudz, const double *kz_im, int Nx, int Nz)
+{
+    const int ign = Nx + 2;
+    for (int k = 1; k <= Nz; k++)
+        for (int i = 0; i <= Nx / 2; i++)
+            mul_ik(kz_im[k - 1], u + 2 * i + (size_t)ign * (k - 1), dudz + 2 * i + (size_t)ign * (k - 1));
+}
+
 /* omega_x at the v faces as nonlinear() forms it before stats()
- * (FOU3D.f90:314-338): u2 placed in Nspec-sized planes by
- * modes_to_planes_phys (FOU3D.f90:816-860: dk_phys = 0, planes 0..nyv+1),
- * der_z_N (FOU3D.f90:525-546, no masking), der_yv_h_wx (FOU3D.f90:592-610)
- * placed the same way, -wx + du3dy over planes 0..nyu+1 (FOU3D.f90:331-336)
- * and four_to_phys_N (FOU3D.f90:700-714: cft then rft of the Nspec sizes, no
- * row zeroed).  Plane nyu+1, which the transposes never write, holds zeros.
+ * (FOU3D.f90:314-338), plane by plane: u2PLN = 0 and modes_to_planes_phys
+ * of u2 (FOU3D.f90:816-860: dk_phys = 0, planes 0..nyv+1), der_z_N with
+ * k1F_z, der_yv_h_wx (FOU3D.f90:592-610) placed the same way, wx = -wx +
+ * du3dy over planes 0..nyu+1 (FOU3D.f90:331-336) and four_to_phys_N
+ * (FOU3D.f90:700-714: cft then rft of the Nspec sizes, no row zeroed).
+ * Plane nyu+1, which the transposes never write, holds zeros.
  * wx: (nyu+2) planes of (Nx+2) x Nz reals. */
 void lho_omega_x(lho_ctx *c, double *wx)
 {
@@ -1310,29 +1321,33 @@ void lho_omega_x(lho_ctx *c, double *wx)
     const int nwork = 4 * (Nx > Nz ? Nx : Nz) + 8;
 #pragma omp parallel num_threads(c->nthr)
     {
-        double *w = zalloc(nwork);
+        double *w = zalloc(nwork), *u2pl = zalloc(plane), *dy = zalloc(plane);
 #pragma omp for schedule(static)
         for (int j = 0; j <= nyu + 1; j++) {
             double *P = wx + plane * j;
-            memset(P, 0, plane * sizeof(double));
+            memset(u2pl, 0, plane * sizeof(double));
+            memset(dy, 0, plane * sizeof(double));
             if (j <= nyv + 1) {
                 const double dth = c->dthdyv[j];
                 for (int col = 1; col <= c->ncols; col++) {
                     const int i = c->col_i[col], k = c->col_k[col];
                     const double *v = CX(c->u2, 0, lv, j, col);
                     const double *a = CX(c->u3, 0, lu, j + 1, col), *b = CX(c->u3, 0, lu, j, col);
-                    double dz[2];
-                    mul_ik(c->k1z[k - 1], v, dz);
-                    const double dy0 = (a[0] - b[0]) * dth * c->ddthetavi;
-                    const double dy1 = (a[1] - b[1]) * dth * c->ddthetavi;
-                    P[2 * i + (size_t)ign * (k - 1)] = -dz[0] + dy0;
-                    P[2 * i + 1 + (size_t)ign * (k - 1)] = -dz[1] + dy1;
+                    const size_t o = 2 * (size_t)i + (size_t)ign * (k - 1);
+                    u2pl[o] = v[0];
+                    u2pl[o + 1] = v[1];
+                    dy[o] = (a[0] - b[0]) * dth * c->ddthetavi;
+                    dy[o + 1] = (a[1] - b[1]) * dth * c->ddthetavi;
                 }
             }
+            lho_der_z_n(u2pl, P, c->k1z, Nx, Nz);
+            for (size_t e = 0; e < plane; e++) P[e] = -P[e] + dy[e];
             lho_cft(P, ign, 2, (Nx + 2) / 2, 1, &c->czN, w);
             lho_rft(P, ign, Nz, 1, &c->rxN, w);
         }
         free(w);
+        free(u2pl);
+        free(dy);
     }
 }
 

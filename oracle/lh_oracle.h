@@ -139,6 +139,9 @@ void lho_stats(lho_ctx *c, double *acc);
 /* ppPL <- p as nonlinear() does at output steps (FOU3D.f90:149-152); the
  * snapshot is zero until the first call */
 void lho_pressure_snapshot(lho_ctx *c);
+/* der_z_N (FOU3D.f90:525-546) on an (Nx+2) x Nz real plane viewed as complex
+ * (0:Nx/2, Nz): dudz = kz(k) u with kz_im the imaginary parts of kz(1:Nz) */
+void lho_der_z_n(const double *u, double *dudz, const double *kz_im, int Nx, int Nz);
 /* omega_x of the current state at planes 0..nyu+1 (FOU3D.f90:314-338):
  * (nyu+2) planes of (Nx+2) x Nz reals, physical values at i = 1..Nx */
 void lho_omega_x(lho_ctx *c, double *wx);

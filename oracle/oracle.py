@@ -89,6 +89,7 @@ def lib(threaded: bool = False) -> ctypes.CDLL:
     L.lho_stats.argtypes = [v, dp]
     L.lho_pressure_snapshot.argtypes = [v]
     L.lho_omega_x.argtypes = [v, dp]
+    L.lho_der_z_n.argtypes = [dp, dp, dp, i, i]
     L.lho_cfft_init.restype = i
     L.lho_rfft_init.restype = i
     _libs[threaded] = L
@@ -372,3 +373,15 @@ def read_in_np1(dirin: str, tag: str, Nx: int, Nz: int, nyu: int, nyv: int):
     for j in range(1, nyu + 1):
         p[:, j - 1] = plane_to_columns(fp.planes[j], Nx, Nz)
     return u1, u2, u3, p, f1
+
+
+def der_z_n(u: np.ndarray, kz_im, Nx: int, Nz: int, threaded: bool = False) -> np.ndarray:
+    """der_z_N (FOU3D.f90:525-546) on an (Nx+2) x Nz real plane [k][i]: kz(k) u
+    on every complex entry; kz_im are the imaginary parts of kz(1:Nz)."""
+    L = lib(threaded)
+    u = np.ascontiguousarray(u, dtype=np.float64).reshape(Nz, Nx + 2)
+    out = np.zeros_like(u)
+    kz = np.ascontiguousarray(kz_im, dtype=np.float64)
+    L.lho_der_z_n(_dp(u), _dp(out), _dp(kz), Nx, Nz)
+    return out
+

@@ -4,7 +4,8 @@
   input files bit for bit (tests/golden/grid_ny153_dyq10_p5.npz).
 * der_x / der_z masks (FOU3D.f90:420-523), checked against an independent
   statement of the rule and a literal table for the fill pattern of
-  test_der_x.f90:20-24 (u(i,k) = 100 k + i).
+  test_der_x.f90:20-24 (u(i,k) = 100 k + i); der_z_N (FOU3D.f90:525-546)
+  against the case of test_der_z.f90 (u(i,k) = 10 k + i, kz = i, 2i).
 * After a full RK3 step from the reference's 32x32x153 initial condition the
   projected field is divergence-free to round-off (error(), littleharsh.f90:
   370-409) and the time step follows the CFL rule (FOU3D.f90:290-303).
@@ -84,6 +85,17 @@ def test_der_x_literal_table():
     assert np.array_equal(d, expect)
     assert d[1, 2:4].tolist() == [-203.0, 202.0]       # row 2, i = 1
     assert d[4].tolist() == [0.0] * 8                   # row 5: kz = -Nz/2 zeroed
+
+
+def test_der_z_n_literal_table():
+    """test_der_z.f90: Nspec_x = 4, Nspec_z = 2, u(i,k) = 10k + i packed real,
+    kz = (0,1), (0,2): dudz = kz u on every complex entry (der_z_N,
+    FOU3D.f90:525-546, no masking)."""
+    u = np.array([[10.0 * k + i for i in range(1, 7)] for k in (1, 2)])
+    d = O.der_z_n(u, [1.0, 2.0], 4, 2)
+    expect = np.array([[-12.0, 11.0, -14.0, 13.0, -16.0, 15.0],
+                       [-44.0, 42.0, -48.0, 46.0, -52.0, 50.0]])
+    assert np.array_equal(d, expect)
 
 
 def test_one_step_from_reference_ic(golden_dir):
