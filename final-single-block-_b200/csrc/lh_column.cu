@@ -530,6 +530,443 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
 }
 
 // ---------------------------------------------------------------------------
+// Column pass for small mode counts: one CTA per column, the y rows spread
+// over the lanes.  With few columns the sequential sweeps of k_column leave
+// most SMs idle and the step waits on the per-row latency of 154-row
+// recurrences; here every recurrence of the column pass -- the Helmholtz LU
+// factors (a continued fraction), the forward and back substitutions and the
+// LUsolP sweeps -- is a chain of per-row maps, each lane composes the maps of
+// its block of rows, a warp scan (5 shuffle steps) gives every lane the value
+// entering its block, and the lane then runs its rows with the reference's
+// per-row arithmetic.  Only the values at block boundaries are formed in a
+// different order (rounding differences of a few ulp; the per-row operations
+// are the sequential ones).  The column's fields stay in shared memory
+// between the phases, so besides the state only Nu and p are written.
+// x -> (a x + b) / (c x + d), the LU-factor step a3u' = a3 / (a2 - a1 a3u)
+struct Mob {
+    double a, b, c, d;
+};
+__device__ __forceinline__ Mob mob_then(const Mob &m, const Mob &n)  // m after n
+{
+    Mob r{m.a * n.a + m.b * n.c, m.a * n.b + m.b * n.d, m.c * n.a + m.d * n.c, m.c * n.b + m.d * n.d};
+    // rescale by a power of two (exact) so long products stay in range
+    const double sc = fmax(fmax(fabs(r.a), fabs(r.b)), fmax(fabs(r.c), fabs(r.d)));
+    if (sc > 0.0 && isfinite(sc)) {
+        int e;
+        frexp(sc, &e);
+        r.a = ldexp(r.a, -e);
+        r.b = ldexp(r.b, -e);
+        r.c = ldexp(r.c, -e);
+        r.d = ldexp(r.d, -e);
+    }
+    return r;
+}
+// y -> A + B y with complex A, real B (forward and back substitutions)
+struct Aff {
+    double2 A;
+    double B;
+};
+__device__ __forceinline__ Aff aff_then(const Aff &m, const Aff &n)  // m after n
+{
+    return Aff{make_double2(m.A.x + m.B * n.A.x, m.A.y + m.B * n.A.y), m.B * n.B};
+}
+__device__ __forceinline__ Mob shfl_mob(const Mob &m, int o, bool up)
+{
+    Mob r;
+    r.a = up ? __shfl_up_sync(0xffffffffu, m.a, o) : __shfl_down_sync(0xffffffffu, m.a, o);
+    r.b = up ? __shfl_up_sync(0xffffffffu, m.b, o) : __shfl_down_sync(0xffffffffu, m.b, o);
+    r.c = up ? __shfl_up_sync(0xffffffffu, m.c, o) : __shfl_down_sync(0xffffffffu, m.c, o);
+    r.d = up ? __shfl_up_sync(0xffffffffu, m.d, o) : __shfl_down_sync(0xffffffffu, m.d, o);
+    return r;
+}
+__device__ __forceinline__ Aff shfl_aff(const Aff &m, int o, bool up)
+{
+    Aff r;
+    r.A.x = up ? __shfl_up_sync(0xffffffffu, m.A.x, o) : __shfl_down_sync(0xffffffffu, m.A.x, o);
+    r.A.y = up ? __shfl_up_sync(0xffffffffu, m.A.y, o) : __shfl_down_sync(0xffffffffu, m.A.y, o);
+    r.B = up ? __shfl_up_sync(0xffffffffu, m.B, o) : __shfl_down_sync(0xffffffffu, m.B, o);
+    return r;
+}
+// Exclusive scans over the lanes: what enters lane l's block is the
+// composition of the blocks before it (ascending rows) or after it
+// (descending rows).
+__device__ __forceinline__ Mob scan_mob_excl(Mob m, int lane)
+{
+    for (int o = 1; o < 32; o <<= 1) {
+        const Mob other = shfl_mob(m, o, true);
+        if (lane >= o) m = mob_then(m, other);
+    }
+    Mob e = shfl_mob(m, 1, true);
+    if (lane == 0) e = Mob{1.0, 0.0, 0.0, 1.0};
+    return e;
+}
+__device__ __forceinline__ Aff scan_aff_excl(Aff m, int lane, bool ascending)
+{
+    for (int o = 1; o < 32; o <<= 1) {
+        const Aff other = shfl_aff(m, o, ascending);
+        if (ascending ? lane >= o : lane + o < 32) m = aff_then(m, other);
+    }
+    Aff e = shfl_aff(m, 1, ascending);
+    if (ascending ? lane == 0 : lane == 31) e = Aff{make_double2(0.0, 0.0), 1.0};
+    return e;
+}
+
+// Helmholtz rows of one grid (solveU's LU_build, tridLU_3D.f90:163-221):
+// row 0 [0, 1, w0], rows 1..n [-beta d1, 1 - beta (d2 + k2), -beta d3],
+// row n+1 [wt, 1, 0]
+struct HRow {
+    double a1, a2, a3;
+};
+__device__ __forceinline__ HRow helm_row(int j, int n, const double *d, double beta, double k2x, double k2z,
+                                         double w0, double wt)
+{
+    if (j == 0) return HRow{0.0, 1.0, w0 * 1.0};
+    if (j == n + 1) return HRow{wt, 1.0, 0.0};
+    return HRow{-beta * d[3 * j], 1.0 - beta * (d[3 * j + 1] + k2x + k2z), -beta * d[3 * j + 2]};
+}
+
+// LU factors of one grid's Helmholtz matrix for rows 0..n+1 into fac
+// (a3u, the scaled upper diagonal) and inv (the inverse pivot), one warp.
+__device__ void small_factors(int lane, int n, const double *d, double beta, double k2x, double k2z, double w0,
+                              double wt, double *fac, double *inv)
+{
+    const int rows = n + 2, K = (rows + 31) / 32, r0 = lane * K, r1 = min(rows, r0 + K);
+    Mob m{1.0, 0.0, 0.0, 1.0};
+    for (int j = r0; j < r1; j++) {
+        const HRow h = helm_row(j, n, d, beta, k2x, k2z, w0, wt);
+        m = mob_then(Mob{0.0, h.a3, -h.a1, h.a2}, m);
+    }
+    const Mob e = scan_mob_excl(m, lane);
+    double x = e.b / e.d;  // a3u entering the block (the block of row 0 ignores it)
+    for (int j = r0; j < r1; j++) {
+        const HRow h = helm_row(j, n, d, beta, k2x, k2z, w0, wt);
+        const double iv = 1.0 / (h.a2 - h.a1 * x);
+        x = h.a3 * iv;
+        inv[j] = iv;
+        fac[j] = x;
+    }
+}
+
+// Forward and back substitution of one Helmholtz system, one warp: rh holds
+// the right-hand side (rows 0 and n+1: zero) and receives the solution.
+__device__ void small_solve(int lane, int n, const double *d, double beta, double k2x, double k2z, double w0,
+                            double wt, const double *fac, const double *inv, double2 *rh)
+{
+    const int rows = n + 2, K = (rows + 31) / 32, r0 = lane * K, r1 = min(rows, r0 + K);
+    // forward: y_j = (rh_j - a1_j y_{j-1}) inv_j
+    Aff m{make_double2(0.0, 0.0), 1.0};
+    for (int j = r0; j < r1; j++) {
+        const double a1 = helm_row(j, n, d, beta, k2x, k2z, w0, wt).a1, iv = inv[j];
+        const double2 r = rh[j];
+        m = aff_then(Aff{make_double2(r.x * iv, r.y * iv), -(a1 * iv)}, m);
+    }
+    Aff e = scan_aff_excl(m, lane, true);
+    double2 yp = e.A;
+    for (int j = r0; j < r1; j++) {
+        const double a1 = helm_row(j, n, d, beta, k2x, k2z, w0, wt).a1, iv = inv[j];
+        const double2 r = rh[j];
+        yp = make_double2((r.x - a1 * yp.x) * iv, (r.y - a1 * yp.y) * iv);
+        rh[j] = yp;
+    }
+    __syncwarp();
+    // back: u_j = y_j - fac_j u_{j+1} (fac of row n+1 is zero)
+    m = Aff{make_double2(0.0, 0.0), 1.0};
+    for (int j = r1 - 1; j >= r0; j--) m = aff_then(Aff{rh[j], -fac[j]}, m);
+    e = scan_aff_excl(m, lane, false);
+    double2 v = e.A;
+    for (int j = r1 - 1; j >= r0; j--) {
+        const double2 y = rh[j];
+        const double f = fac[j];
+        v = make_double2(y.x - f * v.x, y.y - f * v.y);
+        rh[j] = v;
+    }
+    __syncwarp();
+}
+
+size_t column_small_smem_bytes(int max_nyu)
+{
+    const size_t R = (size_t)max_nyu + 2;
+    // double2 rows: old u1 u3 u2, solved u1 u3 u2, psi, p; doubles: the two
+    // grids' factors and pivots, DG2, DG3, and the y metrics (d2/dy2 of both
+    // grids, dtheta/dy of both grids, DG1)
+    return 8 * R * sizeof(double2) + 15 * R * sizeof(double);
+}
+
+__global__ void __launch_bounds__(32 * kSmallWarps) k_column_small(const Inst *__restrict__ insts,
+                                                                   const Work *__restrict__ work, int kRK)
+{
+    extern __shared__ double2 sbuf[];
+    const Work w = work[blockIdx.x];
+    const Inst &I = insts[w.inst];
+    const int col = w.j, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nc = I.nc, nxh = I.nxh, nyu = I.nyu, nyv = I.nyv, R = nyu + 2, Rv = nyv + 2;
+    const int i = col % nxh, kr = col / nxh;
+    const RK rk = rk_coeffs(kRK);
+    const double dt = I.sc[SC_DT];
+    const double Re = I.Re;
+    const double C1 = rk.a / Re, C2 = -rk.c, G = -rk.g;
+    const double kxr = I.kx[i], kzr = I.kz[kr];
+    const double k2x = I.k2x[i], k2z = I.k2z[kr];
+    const double beta = rk.b * dt / Re;
+    const double ddv = I.ddthetavi;
+    const bool mean = (col == 0);
+    double2 *U1 = I.U1 + col, *U2 = I.U2 + col, *U3 = I.U3 + col, *P = I.P + col;
+    // shared layout, R = nyu+2 rows per array (the v grid uses Rv = R-1);
+    // rows of fields stored from j = 1 sit at index j-1
+    double2 *O1 = sbuf, *O3 = O1 + R, *O2 = O3 + R;      // state before the substep
+    double2 *S1 = O2 + R, *S3 = S1 + R, *S2 = S3 + R;    // right-hand sides -> solutions
+    double2 *PS = S2 + R;                                 // psi, rows 1..nyu
+    double2 *SP = PS + R;                                 // p, rows 1..nyu
+    double *facu = reinterpret_cast<double *>(SP + R), *invu = facu + R, *facv = invu + R, *invv = facv + R;
+    double *SG2 = invv + R, *SG3 = SG2 + R;               // DG2, DG3, rows 1..nyu
+
+    // Stage the column and the y metrics: every load of a row is issued
+    // before its stores.  The loads go through the read-only path: a CTA
+    // reads only its own column here, before any of its writes.
+    double *du = SG3 + R, *dv = du + 3 * R, *thu = dv + 3 * R, *thv = thu + R, *dg1 = thv + R;  // y metrics
+    const double2 z2 = make_double2(0.0, 0.0);
+    for (int j = threadIdx.x; j < R; j += blockDim.x) {
+        const size_t o = (size_t)j * nc + col;
+        const bool v = j < Rv, pr = j < nyu;
+        const double2 a1 = __ldg(I.U1 + o), a3 = __ldg(I.U3 + o), a2 = v ? __ldg(I.U2 + o) : z2;
+        const double2 pp = pr ? __ldg(I.P + o) : z2;
+        const double g2 = pr ? __ldg(I.DG2 + o) : 0.0, g3 = pr ? __ldg(I.DG3 + o) : 0.0;
+        const double m0 = __ldg(I.dyu2i + 3 * j), m1 = __ldg(I.dyu2i + 3 * j + 1), m2 = __ldg(I.dyu2i + 3 * j + 2);
+        const double e0 = v ? __ldg(I.dyv2i + 3 * j) : 0.0, e1 = v ? __ldg(I.dyv2i + 3 * j + 1) : 0.0;
+        const double e2 = v ? __ldg(I.dyv2i + 3 * j + 2) : 0.0;
+        const double tu = __ldg(I.dthdyu + j), tv = v ? __ldg(I.dthdyv + j) : 0.0;
+        const double d1 = j < nyu + 1 ? __ldg(I.DG1 + j) : 0.0;
+        O1[j] = a1;
+        O3[j] = a3;
+        du[3 * j] = m0;
+        du[3 * j + 1] = m1;
+        du[3 * j + 2] = m2;
+        thu[j] = tu;
+        if (j < nyu + 1) dg1[j] = d1;
+        if (v) {
+            O2[j] = a2;
+            dv[3 * j] = e0;
+            dv[3 * j + 1] = e1;
+            dv[3 * j + 2] = e2;
+            thv[j] = tv;
+        }
+        if (pr) {
+            SP[j] = pp;
+            SG2[j] = g2;
+            SG3[j] = g3;
+        }
+    }
+    __syncthreads();
+    // LU factors (u grid by warp 0, shared by the u1 and u3 chains, which
+    // form identical factors in the reference; v grid by warp 2)
+    if (warp == 0) small_factors(lane, nyu, du, beta, k2x, k2z, I.gw1, I.gw2, facu, invu);
+    if (warp == 2) small_factors(lane, nyv, dv, beta, k2x, k2z, 0.0, 0.0, facv, invv);
+    __syncthreads();
+
+    // ---- right-hand sides (RHS0, Nu sum, du += -g Nu, solveU rhs) --------
+    if (warp < 2) {
+        const int role = warp;
+        const double2 *O = role == 0 ? O1 : O3;
+        const double2 *SN = (role == 0 ? I.NU1 : I.NU3) + col, *SX = (role == 0 ? I.NXZ1 : I.NXZ3) + col;
+        const double2 *FL = (role == 0 ? I.UVF : I.WVF) + col;
+        double2 *S = role == 0 ? S1 : S3;
+        double2 *N = (role == 0 ? I.NU1 : I.NU3) + col;
+        const double dC3 = rk.d * (role == 0 ? kxr : kzr);
+        const double C1m = (role == 0 && mean) ? -rk.d * I.sc[SC_MPGX] : 0.0;
+        for (int j = lane; j < R; j += 32) {
+            if (j == 0 || j == nyu + 1) {
+                S[j] = make_double2(0.0, 0.0);
+                continue;
+            }
+            const double2 um = O[j - 1], uc = O[j], up = O[j + 1];
+            const size_t o = (size_t)j * nc, on = o - nc;
+            // Nu_old is overwritten below in this iteration: a plain load
+            const double2 no = SN[on], x = __ldg(SX + on), fl = __ldg(FL + o), flp = __ldg(FL + on);
+            const double2 pj = SP[j - 1];
+            const double d1 = du[3 * j], d2 = du[3 * j + 1], d3 = du[3 * j + 2];
+            const double cen = k2x + k2z + d2;
+            const double2 L = make_double2(d1 * um.x + cen * uc.x + d3 * up.x, d1 * um.y + cen * uc.y + d3 * up.y);
+            double2 dd = make_double2(C1 * L.x + C2 * no.x + dC3 * pj.y, C1 * L.y + C2 * no.y + -(dC3 * pj.x));
+            if (role == 0 && mean) dd.x = dd.x + C1m;
+            const double m = thu[j];
+            const double2 nu = make_double2(x.x + (fl.x - flp.x) * m * ddv, x.y + (fl.y - flp.y) * m * ddv);
+            N[(size_t)(j - 1) * nc] = nu;
+            dd = make_double2(dd.x + G * nu.x, dd.y + G * nu.y);
+            S[j] = make_double2(uc.x + dt * dd.x, uc.y + dt * dd.y);
+        }
+        __syncwarp();
+        small_solve(lane, nyu, du, beta, k2x, k2z, I.gw1, I.gw2, facu, invu, S);
+    } else {
+        double2 *N = I.NU2 + col;
+        const double2 *SN2 = I.NU2 + col, *SX2 = I.NXZ2 + col, *SVV = I.VVC + col;
+        for (int j = lane; j < Rv; j += 32) {
+            if (j == 0 || j == nyv + 1) {
+                S2[j] = make_double2(0.0, 0.0);
+                continue;
+            }
+            const double2 um = O2[j - 1], uc = O2[j], up = O2[j + 1];
+            const size_t o = (size_t)j * nc, on = o - nc;
+            // Nu_old is overwritten below in this iteration: a plain load
+            const double2 no = SN2[on], x = __ldg(SX2 + on), vvc = __ldg(SVV + o), vvn = __ldg(SVV + o + nc);
+            const double2 pc = SP[j - 1], pn = SP[j];
+            const double e1 = dv[3 * j], e2 = dv[3 * j + 1], e3 = dv[3 * j + 2];
+            const double cenv = k2x + k2z + e2;
+            const double2 L = make_double2(e1 * um.x + cenv * uc.x + e3 * up.x, e1 * um.y + cenv * uc.y + e3 * up.y);
+            const double mv = thv[j];
+            const double C3 = -rk.d * ddv * mv;
+            double2 dd = make_double2(C1 * L.x + C2 * no.x + C3 * (pn.x - pc.x), C1 * L.y + C2 * no.y + C3 * (pn.y - pc.y));
+            const double2 nu = make_double2(x.x + (vvn.x - vvc.x) * mv * ddv, x.y + (vvn.y - vvc.y) * mv * ddv);
+            N[(size_t)(j - 1) * nc] = nu;
+            dd = make_double2(dd.x + G * nu.x, dd.y + G * nu.y);
+            S2[j] = make_double2(uc.x + dt * dd.x, uc.y + dt * dd.y);
+        }
+        __syncwarp();
+        small_solve(lane, nyv, dv, beta, k2x, k2z, 0.0, 0.0, facv, invv, S2);
+    }
+    __syncthreads();
+
+    const double dtirk = (1.0 / dt) / (rk.a + rk.b);
+    if (I.flag_ctpress == 0 && mean && threadIdx.x == 0) {
+        // flowrate_corr (littleharsh.f90:515-548), as in k_column
+        double *u11 = I.U11, *f11 = I.F11;
+        const int ne = nyu + 1;
+        const double bdt = -rk.d * dt;
+        double a3p = I.gw1 * 1.0;
+        double yp = 0.0 * 1.0;
+        u11[0] = yp;
+        f11[0] = a3p;
+        for (int j = 1; j <= ne; j++) {
+            double a1, a2, a3, rr;
+            if (j < ne) {
+                a1 = -beta * du[3 * j];
+                a2 = 1.0 - beta * du[3 * j + 1];
+                a3 = -beta * du[3 * j + 2];
+                rr = bdt;
+            } else {
+                a1 = I.gw2;
+                a2 = 1.0;
+                a3 = 0.0;
+                rr = 0.0;
+            }
+            const double inv = 1.0 / (a2 - a1 * a3p);
+            yp = (rr - a1 * yp) * inv;
+            a3p = a3 * inv;
+            u11[j] = yp;
+            f11[j] = a3p;
+        }
+        double up = yp;
+        for (int j = ne - 1; j >= 0; j--) {
+            up = u11[j] - f11[j] * up;
+            u11[j] = up;
+        }
+        double Qx1 = 0.0, Qx0 = 0.0;
+        for (int j = 1; j <= nyv + 1; j++) Qx1 = Qx1 + (I.yv[j] - I.yv[j - 1]) * u11[j - 1];
+        for (int j = 1; j <= nyv + 1; j++) Qx0 = Qx0 + (I.yv[j] - I.yv[j - 1]) * S1[j].x;
+        const double g = (I.sc[SC_QXT] - Qx0) / Qx1;
+        I.sc[SC_MPGX] = I.sc[SC_MPGX] + g;
+        I.sc[SC_DGX] = g;
+        for (int j = 0; j <= ne; j++) S1[j].x = S1[j].x + g * u11[j];
+    }
+    __syncthreads();
+
+    // ---- divergence and LUsolP (warp 0), p += psi ------------------------
+    if (warp == 0) {
+        const int K = (nyu + 31) / 32, r0 = 1 + lane * K, r1 = min(nyu + 1, r0 + K);
+        // psi = div / (dt (a+b)) into PS; forward x_j = (ps_j - g1_j x_{j-1}) g2_j, x_0 = 0
+        Aff m{make_double2(0.0, 0.0), 1.0};
+        for (int j = r0; j < r1; j++) {
+            const double2 a = S1[j], c3 = S3[j], v2c = S2[j], v2m = S2[j - 1];
+            const double mm = ddv * thu[j];
+            const double2 d = make_double2(-(kxr * a.y) + -(kzr * c3.y) + mm * (v2c.x - v2m.x),
+                                           kxr * a.x + kzr * c3.x + mm * (v2c.y - v2m.y));
+            double2 ps = cscale(dtirk, d);
+            if (mean && j == 1) ps = make_double2(0.0, 0.0);
+            PS[j - 1] = ps;
+            const double g2 = SG2[j - 1], g1 = j == 1 ? 0.0 : dg1[j];
+            m = aff_then(Aff{make_double2(ps.x * g2, ps.y * g2), -(g1 * g2)}, m);
+        }
+        Aff e = scan_aff_excl(m, lane, true);
+        double2 xp = e.A;
+        for (int j = r0; j < r1; j++) {
+            const double2 ps = PS[j - 1];
+            const double g2 = SG2[j - 1];
+            if (j == 1) xp = cscale(g2, ps);
+            else {
+                const double g1 = dg1[j];
+                xp = make_double2((ps.x - g1 * xp.x) * g2, (ps.y - g1 * xp.y) * g2);
+            }
+            PS[j - 1] = xp;
+        }
+        __syncwarp();
+        // back: psi_j = x_j - g3_j psi_{j+1} (psi_nyu = x_nyu); p += psi
+        m = Aff{make_double2(0.0, 0.0), 1.0};
+        for (int j = r1 - 1; j >= r0; j--) {
+            const double g3 = j < nyu ? SG3[j - 1] : 0.0;
+            m = aff_then(Aff{PS[j - 1], -g3}, m);
+        }
+        e = scan_aff_excl(m, lane, false);
+        double2 psn = e.A;
+        for (int j = r1 - 1; j >= r0; j--) {
+            const double2 x = PS[j - 1];
+            double2 ps = x;
+            if (j < nyu) {
+                const double g3 = SG3[j - 1];
+                ps = make_double2(x.x - g3 * psn.x, x.y - g3 * psn.y);
+            }
+            PS[j - 1] = ps;
+            const double2 pv = SP[j - 1];
+            P[(size_t)(j - 1) * nc] = make_double2(pv.x + ps.x, pv.y + ps.y);
+            psn = ps;
+        }
+    }
+    __syncthreads();
+
+    // ---- v_corr and the ghost rows (littleharsh.f90:896-993) -------------
+    const double dtrk = dt * (rk.a + rk.b);
+    if (warp < 2) {
+        const int role = warp;
+        double2 *S = role == 0 ? S1 : S3;
+        double2 *U = role == 0 ? U1 : U3;
+        const double kd = dtrk * (role == 0 ? kxr : kzr);
+        for (int j = 1 + lane; j <= nyu; j += 32) {
+            const double2 ps = PS[j - 1];
+            double2 a = S[j];
+            a = make_double2(a.x - -(kd * ps.y), a.y - kd * ps.x);
+            S[j] = a;
+            U[(size_t)j * nc] = a;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            const double2 first = S[1], last = S[nyu], ps1 = PS[0];
+            U[0] = cscale(I.gwbc, first);
+            U[(size_t)(nyu + 1) * nc] = cscale(I.gwbc, last);
+            if (!isfinite(first.x) || !isfinite(first.y) || !isfinite(ps1.x) || !isfinite(ps1.y))
+                atomicOr(I.err, ERR_NONFINITE);
+            if (role == 0 && mean && kRK == 3) {
+                // flowrateIm (littleharsh.f90:473-492) via meanflow_ctP (:572-589)
+                double Qu = 0.0;
+                for (int j = 1; j <= nyv + 1; j++) Qu = Qu + (I.yv[j] - I.yv[j - 1]) * S1[j].x;
+                I.sc[SC_QX] = Qu;
+                I.sc[SC_ITER] = I.sc[SC_ITER] + 1.0;
+            }
+        }
+    } else {
+        const double dtrk_u2 = dtrk * ddv;
+        for (int j = 1 + lane; j <= nyv; j += 32) {
+            const double2 psc = PS[j - 1], psn = PS[j];
+            const double mv = dtrk_u2 * thv[j];
+            double2 v = S2[j];
+            v = make_double2(v.x - mv * (psn.x - psc.x), v.y - mv * (psn.y - psc.y));
+            U2[(size_t)j * nc] = v;
+        }
+        if (lane == 0) {
+            U2[0] = make_double2(0.0, 0.0);
+            U2[(size_t)(nyv + 1) * nc] = make_double2(0.0, 0.0);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // dt at kRK = 1 (FOU3D.f90:290-303).  CFL mode folds the spectral wall plane
 // 0 of u1/u3 (which dtc_calc scans as raw coefficients, its explicit-shape
 // dummies starting one plane early) into the maxima the plane pipeline

@@ -269,6 +269,10 @@ cudaError_t instance_download(DevInstance &d, double *u1, double *u2, double *u3
     return cudaStreamSynchronize(st);
 }
 
+// Plans with at most this many columns in all use the one-CTA-per-column
+// column pass (LH_SMALL_COLUMNS overrides).
+constexpr long kSmallColumnsDefault = 1536;
+
 // ---------------------------------------------------------------------------
 namespace {
 struct ClassTiles {
@@ -387,6 +391,14 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
         chunk_eff[q] = (int)c;
         rounds = std::max(rounds, (s.nyu + chunk_eff[q] - 1) / chunk_eff[q]);
     }
+    // The column pass: with few columns in the plan, one CTA per column with
+    // the rows spread over its lanes (k_column_small); otherwise 32 columns
+    // per CTA, one lane each (k_column).
+    size_t total_cols = 0;
+    for (const DevInstance *d : insts) total_cols += (size_t)d->hs.nc;
+    const char *sc = getenv("LH_SMALL_COLUMNS");
+    const long small_max = sc ? atol(sc) : kSmallColumnsDefault;
+    p.col_small = (long)total_cols <= small_max;
     // work lists [round][stage][class]
     std::vector<std::vector<std::vector<std::vector<Work>>>> lists(
         rounds, std::vector<std::vector<std::vector<Work>>>(3, std::vector<std::vector<Work>>(ncls)));
@@ -428,7 +440,10 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
                 for (int b = 0; b < nbf; b++) L[2][cls_of[q]].push_back({q, j, slot, b, 0});
             }
         }
-        for (int b = 0; b < (s.nc + kColumnThreads - 1) / kColumnThreads; b++) p.column.push_back({q, b, 0, 0, 0});
+        if (p.col_small)
+            for (int c = 0; c < s.nc; c++) p.column.push_back({q, c, 0, 0, 0});
+        else
+            for (int b = 0; b < (s.nc + kColumnThreads - 1) / kColumnThreads; b++) p.column.push_back({q, b, 0, 0, 0});
     }
     std::vector<Work> all;
     p.rounds.assign(rounds, {});
@@ -491,6 +506,10 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
     if (gf && (e = raise_smem_limit((const void *)k_zfwd, gf)) != cudaSuccess) return e;
     int max_nyu = 1;
     for (const DevInstance *d : insts) max_nyu = std::max(max_nyu, d->hs.nyu);
+    if (p.col_small) {
+        p.sm_col = column_small_smem_bytes(max_nyu);
+        return raise_smem_limit((const void *)k_column_small, p.sm_col);
+    }
     p.sm_col = column_smem_bytes(max_nyu);
     return raise_smem_limit((const void *)k_column, p.sm_col);
 }
@@ -575,7 +594,11 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
         if ((e = time_end(timer, 3, st)) != cudaSuccess) return e;
     }
     time_begin(timer, st);
-    k_column<<<(unsigned)p.column.size(), kColumnBlock, p.sm_col, st>>>(d_insts, p.d_work + p.off_column, kRK);
+    if (p.col_small)
+        k_column_small<<<(unsigned)p.column.size(), 32 * kSmallWarps, p.sm_col, st>>>(d_insts, p.d_work + p.off_column,
+                                                                                      kRK);
+    else
+        k_column<<<(unsigned)p.column.size(), kColumnBlock, p.sm_col, st>>>(d_insts, p.d_work + p.off_column, kRK);
     if ((e = time_end(timer, 4, st)) != cudaSuccess) return e;
     return cudaGetLastError();
 }

@@ -95,6 +95,7 @@ struct Plan {
     size_t work_cap = 0;     // Work entries d_work holds (reused across rebuilds)
     size_t off_column = 0;
     size_t sm_col = 0;
+    bool col_small = false;  // column pass by k_column_small (one CTA per column)
     int ninst = 0;
     bool force_generic = false;
     cudaStream_t side[kRoundStreams - 1] = {};  // rounds r % kRoundStreams != 0

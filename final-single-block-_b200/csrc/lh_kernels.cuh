@@ -8,6 +8,10 @@ namespace lh {
 constexpr int kColumnThreads = 32;       // columns per column-pass CTA (one lane each)
 constexpr int kColumnBlock = 3 * kColumnThreads;  // three warps: the u1, u3 and u2 chains
 size_t column_smem_bytes(int max_nyu);  // ring + staged y metrics
+// column pass for small mode counts: one CTA of kSmallWarps warps (the u1,
+// u3, u2 chains) per column, rows spread over the lanes
+constexpr int kSmallWarps = 3;
+size_t column_small_smem_bytes(int max_nyu);
 
 __global__ void k_zinv(const Inst *__restrict__ insts, const Work *__restrict__ work, int bc);
 __global__ void k_xprod(const Inst *__restrict__ insts, const Work *__restrict__ work, int br, int want_max);
@@ -22,6 +26,7 @@ __global__ void k_column(const Inst *__restrict__ insts, const Work *__restrict_
 __global__ void k_dt(const Inst *__restrict__ insts, int ninst);
 __global__ void k_col_to_plane(const double2 *__restrict__ src, double2 *__restrict__ dst, int len, int nc);
 __global__ void k_plane_to_col(const double2 *__restrict__ src, double2 *__restrict__ dst, int len, int nc);
+__global__ void k_column_small(const Inst *__restrict__ insts, const Work *__restrict__ work, int kRK);
 __global__ void k_lusolu(const Inst *__restrict__ insts, int grid, int kRK, double dt, const double2 *rhs,
                          double2 *u, double *fac);
 __global__ void k_lusolp(const Inst *__restrict__ insts, double2 *x);

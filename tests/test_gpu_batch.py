@@ -9,6 +9,14 @@ from helpers import rel_l2
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True)
+def _one_column_kernel(monkeypatch):
+    """A batch of many columns and a lone small instance would otherwise run
+    different column-pass kernels (which agree to round-off, tested in
+    test_gpu_parity.py); batching equivalence is checked with the same one."""
+    monkeypatch.setenv("LH_SMALL_COLUMNS", "0")
+
+
 def _ic(desc, seed):
     from lh_b200 import grids, perturbed_laminar
     yu, yv = grids(desc)

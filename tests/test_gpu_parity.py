@@ -236,3 +236,27 @@ def test_fast_and_generic_fft_paths_agree(N, monkeypatch):
         out.append(e.download())
     for f in FIELDS:
         assert rel_l2(out[0][f], out[1][f]) <= (1e-12 if f == "p" else 1e-13), f
+
+
+@pytest.mark.parametrize("N,ctpress", [(16, 1), (32, 0), (64, 1), (128, 1)])
+def test_small_and_sequential_column_passes_agree(N, ctpress, monkeypatch):
+    """The one-CTA-per-column pass (warp scans over the y rows) and the
+    32-columns-per-CTA sequential pass give the same steps: only the values
+    entering each lane's block of rows are formed in a different order.  Both
+    are forced through LH_SMALL_COLUMNS, whichever the size would pick."""
+    from lh_b200 import Desc, grids, perturbed_laminar
+    d = Desc(Nx=N, Nz=N, ny=97, flag_ctpress=ctpress, dt_mode=1, dt=1e-3)
+    yu, yv = grids(d)
+    ic = perturbed_laminar(d, 7, yu, yv)
+    out = []
+    for limit in ("0", "1000000000"):
+        monkeypatch.setenv("LH_SMALL_COLUMNS", limit)
+        e = _engine(d)
+        e.upload(*ic)
+        e.step(3)
+        e.synchronize()
+        out.append((e.download(), e.scalars()))
+    for f in FIELDS:
+        assert rel_l2(out[0][0][f], out[1][0][f]) <= (1e-12 if f == "p" else 1e-13), f
+    if ctpress == 0:
+        assert abs(out[0][1]["mpgx"] - out[1][1]["mpgx"]) <= 1e-10 * abs(out[0][1]["mpgx"])

@@ -10,6 +10,14 @@ from helpers import rel_l2
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True)
+def _one_column_kernel(monkeypatch):
+    """A mixed batch and a lone small request would otherwise run different
+    column-pass kernels (which agree to round-off, tested in
+    test_gpu_parity.py); the serving equivalence is checked with the same one."""
+    monkeypatch.setenv("LH_SMALL_COLUMNS", "0")
+
+
 def test_each_result_same_alone_and_in_the_mix():
     from lh_b200 import Batch, Desc
     from lh_b200.serve import Request, run_plain, serve
