@@ -5,9 +5,17 @@
 // round rather than N.  Each instance owns its device allocation; admission
 // is checked against an HBM budget.  One RK3 step of the current membership
 // is captured once in a CUDA graph and replayed until membership changes.
+//
+// Instances of at least kIsolateModes Fourier modes (Nx*Nz) keep the GPU
+// busy on their own; sharing launches with others only shrinks their L2
+// staging share and splits their rounds, so each gets its own launch plan
+// (its chunk rounds sized as if alone), while the smaller instances share
+// one plan.  The plans' launches follow one another on the batch stream
+// inside the same captured step.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <memory>
 #include <new>
 #include <string>
@@ -23,7 +31,9 @@ struct lh_batch {
     size_t budget = 0, used = 0;
     std::vector<std::unique_ptr<DevInstance>> slots;  // nullptr = free slot
     std::vector<int> live;                            // slot ids in launch order
-    Plan plan;
+    std::vector<Plan> plans;                          // plan groups (see above)
+    std::vector<int> plan_off;                        // first instance of each group in d_insts
+    std::vector<bool> plan_cfl;                       // a CFL-mode instance in the group
     Inst *d_insts = nullptr;
     size_t d_insts_cap = 0;
     cudaStream_t st = nullptr;
@@ -44,6 +54,7 @@ struct lh_batch {
 };
 
 static constexpr size_t kPoolBlocks = 16;
+static constexpr long kIsolateModes = 128 * 128;  // LH_BATCH_ISOLATE overrides
 
 static void pool_release(lh_batch *b, size_t keep_bytes)
 {
@@ -102,7 +113,7 @@ extern "C" int lh_batch_destroy(lh_batch *b)
     if (!b) return LH_OK;
     if (b->st) cudaStreamSynchronize(b->st);
     drop_graph(b);
-    plan_free(b->plan);
+    for (Plan &p : b->plans) plan_free(p);
     if (b->d_insts) cudaFree(b->d_insts);
     for (auto &s : b->slots)
         if (s) instance_free(*s);
@@ -204,22 +215,34 @@ static int rebuild(lh_batch *b)
     if (!b->dirty) return LH_OK;
     drop_graph(b);
     b->live.clear();
-    std::vector<const DevInstance *> v;
-    std::vector<Inst> hi;
     b->any_cfl = false;
-    int maxMx = 0, maxMz = 0, maxnxh = 0, maxnyu = 0;
+    const char *iso = getenv("LH_BATCH_ISOLATE");
+    const long isolate = iso ? atol(iso) : kIsolateModes;
+    // groups: the shared group of the smaller instances first, then one group
+    // per isolated instance; d_insts holds the instances in that order
+    std::vector<std::vector<int>> groups(1);
     for (size_t k = 0; k < b->slots.size(); k++)
         if (b->slots[k]) {
-            b->live.push_back((int)k);
-            v.push_back(b->slots[k].get());
-            hi.push_back(b->slots[k]->inst);
-            b->any_cfl |= b->slots[k]->desc.dt_mode == LH_DT_CFL;
-            maxMx = std::max(maxMx, b->slots[k]->hs.Mx);
-            maxMz = std::max(maxMz, b->slots[k]->hs.Mz);
-            maxnxh = std::max(maxnxh, b->slots[k]->hs.nxh);
-            maxnyu = std::max(maxnyu, b->slots[k]->hs.nyu);
+            const HostSetup &hs = b->slots[k]->hs;
+            if ((long)hs.Nx * hs.Nz >= isolate) groups.push_back({(int)k});
+            else groups[0].push_back((int)k);
         }
-    if (v.empty()) {
+    if (groups[0].empty()) groups.erase(groups.begin());
+    std::vector<Inst> hi;
+    b->plan_off.clear();
+    b->plan_cfl.clear();
+    for (const auto &g : groups) {
+        b->plan_off.push_back((int)hi.size());
+        bool cfl = false;
+        for (int k : g) {
+            b->live.push_back(k);
+            hi.push_back(b->slots[k]->inst);
+            cfl |= b->slots[k]->desc.dt_mode == LH_DT_CFL;
+        }
+        b->plan_cfl.push_back(cfl);
+        b->any_cfl |= cfl;
+    }
+    if (hi.empty()) {
         b->dirty = false;
         return LH_OK;
     }
@@ -230,16 +253,28 @@ static int rebuild(lh_batch *b)
         b->d_insts_cap = hi.size();
     }
     BCK(cudaMemcpy(b->d_insts, hi.data(), hi.size() * sizeof(Inst), cudaMemcpyHostToDevice), "instance table");
-    BCK(plan_build(b->plan, v), "plan");
+    // plans (their work buffers, streams and events) are kept and rebuilt in place
+    while (b->plans.size() > groups.size()) {
+        plan_free(b->plans.back());
+        b->plans.pop_back();
+    }
+    b->plans.resize(groups.size());
+    for (size_t g = 0; g < groups.size(); g++) {
+        std::vector<const DevInstance *> v;
+        for (int k : groups[g]) v.push_back(b->slots[k].get());
+        BCK(plan_build(b->plans[g], v), "plan");
+    }
     BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal), "capture");
     cudaError_t el = cudaSuccess;
-    for (int k = 1; k <= 3 && el == cudaSuccess; k++) el = launch_substep(b->plan, b->d_insts, k, b->any_cfl, b->st);
-    cudaGraph_t g = nullptr;
-    cudaError_t ee = cudaStreamEndCapture(b->st, &g);
+    for (int k = 1; k <= 3 && el == cudaSuccess; k++)
+        for (size_t g = 0; g < b->plans.size() && el == cudaSuccess; g++)
+            el = launch_substep(b->plans[g], b->d_insts + b->plan_off[g], k, b->plan_cfl[g], b->st);
+    cudaGraph_t gr = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(b->st, &gr);
     if (el != cudaSuccess) return bcuda(b, el, "capture launch");
     if (ee != cudaSuccess) return bcuda(b, ee, "capture end");
-    b->graph = g;
-    BCK(cudaGraphInstantiate(&b->gexec, g, 0), "instantiate");
+    b->graph = gr;
+    BCK(cudaGraphInstantiate(&b->gexec, gr, 0), "instantiate");
     b->dirty = false;
     return LH_OK;
 }

@@ -87,3 +87,24 @@ def test_budget_rejects_admission():
         b.add(d, *_ic(d, 2))
     assert ei.value.code == -3
     assert b.count() == 1
+
+
+def test_isolated_plans_equal_the_shared_plan(monkeypatch):
+    """Instances of 128^2 modes and more get a launch plan of their own
+    (LH_BATCH_ISOLATE sets the threshold); the states do not depend on how
+    the instances are grouped into plans."""
+    from lh_b200 import Batch, Desc
+    descs = [Desc(Nx=32, Nz=32, ny=33, dt_mode=1, dt=1e-3), Desc(Nx=128, Nz=128, ny=33, dt_mode=1, dt=5e-4),
+             Desc(Nx=16, Nz=32, ny=41, dt_mode=0, CFL=0.5)]
+    out = []
+    for iso in ("1", "1000000000"):
+        monkeypatch.setenv("LH_BATCH_ISOLATE", iso)
+        b = Batch()
+        slots = [b.add(d, *_ic(d, 300 + k)) for k, d in enumerate(descs)]
+        b.step(3)
+        b.synchronize()
+        out.append([b.download(s) for s in slots])
+        b.close()
+    for k in range(len(descs)):
+        for f in ("u1", "u2", "u3", "p"):
+            assert rel_l2(out[0][k][f], out[1][k][f]) <= 1e-14, (k, f)
