@@ -20,6 +20,7 @@ N > 1 runs under torchrun, one independent instance per rank (weak scaling).
 from __future__ import annotations
 
 import argparse
+import math
 import json
 import os
 import subprocess
@@ -38,20 +39,24 @@ RE_TAU = 180.0
 MPGX = -3.0675e-3
 
 
-def workload_desc():
+def workload_desc(n: int = 128):
+    """The plain workload: Nx = Nz = n Fourier modes (128: the headline
+    configuration), ny = 153, Re_tau = 180, dt = 5e-4."""
     from lh_b200 import Desc, re_from_retau
-    return Desc(Nx=128, Nz=128, ny=153, Re=re_from_retau(RE_TAU, MPGX), mpgx=MPGX, dt_mode=1, dt=5e-4)
+    return Desc(Nx=n, Nz=n, ny=153, Re=re_from_retau(RE_TAU, MPGX), mpgx=MPGX, dt_mode=1, dt=5e-4)
 
 
 def config_dict(desc, n_gpus):
+    m = 3 * desc.Nx // 2
     return {
-        "workload": "plain drop-in, one channel instance per GPU: Nx=Nz=128 modes (192x192 physical, 3/2 pad), "
-                    "ny=153 polynomial-stretched y (dyq=10, p=5), Re_tau=180, dt=5e-4, RK3, seeded "
+        "workload": f"plain drop-in, one channel instance per GPU: Nx=Nz={desc.Nx} modes ({m}x{m} physical, 3/2 "
+                    "pad), ny=153 polynomial-stretched y (dyq=10, p=5), Re_tau=180, dt=5e-4, RK3, seeded "
                     "perturbed-laminar initial state",
         "Nx": desc.Nx, "Nz": desc.Nz, "ny": desc.ny, "Re": desc.Re, "dt": desc.dt,
         "grid_points": desc.points(), "substeps_per_step": 3,
         "instances_per_gpu": 1, "parallelism": f"replicas x{n_gpus}",
-        "l2": "state and per-substep traffic (~0.45 GB resident) exceed the 126 MB L2; no flush",
+        "l2": ("state and per-substep traffic (~0.45 GB resident) exceed the 126 MB L2; no flush"
+               if desc.Nx >= 128 else "diagnostic size: the state fits in the 126 MB L2 (not the headline workload)"),
     }
 
 
@@ -116,6 +121,35 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def fp64_peak_tflops(n: int = 8192, reps: int = 5) -> float:
+    """FP64 denominator measured on this GPU: a float64 GEMM of n^3 (2 n^3
+    flops), best of `reps`, timed with CUDA events."""
+    import torch
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def fft_flops_per_substep(desc) -> float:
+    """FFT flops of one substep counted as 5 N log2 N per complex transform of
+    length N (2.5 N log2 N per real one): 12 ny [Mz 2.5 Mx log2 Mx + (Nx/2+1)
+    5 Mz log2 Mz] -- twelve 2-D transforms per plane pair, the z transforms
+    pruned to the Nx/2+1 retained x modes."""
+    Mx, Mz = 3 * desc.Nx // 2, 3 * desc.Nz // 2
+    return 12.0 * desc.ny * (Mz * 2.5 * Mx * math.log2(Mx) + (desc.Nx // 2 + 1) * 5.0 * Mz * math.log2(Mz))
+
+
 TRAFFIC_SUMMARY = os.path.join(ROOT, "profiles", "dram_traffic_plain_128x128x153.md")
 
 
@@ -155,9 +189,9 @@ def cpu_rate(desc, sample_steps: int, threads: int):
 
 
 def run_reference(args, rank, world):
-    desc = workload_desc()
     if rank != 0:
         return
+    desc = workload_desc(args.nx)
     threads = os.cpu_count() or 1
     steps = max(1, args.steps)
     warm = max(0, min(args.warmup, 1))
@@ -261,7 +295,7 @@ def run_ours(args, rank, world, local_rank):
     import torch
     from lh_b200 import Engine, grids, perturbed_laminar
     torch.cuda.set_device(local_rank)
-    desc = workload_desc()
+    desc = workload_desc(args.nx)
     yu, yv = grids(desc)
     ic = perturbed_laminar(desc, 20260002 + 1000 * rank, yu, yv)
     e = Engine(desc)
@@ -298,7 +332,8 @@ def run_ours(args, rank, world, local_rank):
     alg = substep_alg_bytes(desc)
     sub_s = ms_max * 1e-3 / (3 * K)  # one substep, from the timed region
     achieved = alg / sub_s / 1e9
-    traffic = ncu_traffic()
+    # the committed ncu summary covers the 128x128x153 workload only
+    traffic = ncu_traffic() if desc.Nx == 128 else {}
     traffic_sub = sum(traffic.values()) if traffic else None
     kernels = {}
     for name, (kms, kn) in prof.items():
@@ -340,6 +375,15 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_serve:
         batched, served = batched_and_served(args)
 
+    fp64 = None
+    if rank == 0 and world == 1:
+        fl = fft_flops_per_substep(desc)
+        pk = fp64_peak_tflops()
+        fp64 = {"kernel": "the FFT flops of one substep (plane pass k_zinv/k_xprod/k_zfwd) over the whole substep time",
+                "achieved": fl / sub_s / 1e12, "peak": pk, "unit": "TFLOP/s", "frac": fl / sub_s / 1e12 / pk,
+                "flops_per_substep": fl,
+                "peak_source": "measured on this GPU: float64 GEMM 8192^3 (torch.matmul), best of 5"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -359,6 +403,7 @@ def run_ours(args, rank, world, local_rank):
                          "achieved": achieved, "peak": hbm, "peak_source": src, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic_sub, "alg_bytes": alg,
                          "avg_duration_ms": sub_s * 1e3},
+            "fp64": fp64,
             "kernels": kernels,
             "dominant_kernel": dom[0],
             "cpu_baseline": cpu,
@@ -378,6 +423,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-serve", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--nx", type=int, default=128,
+                    help="Fourier modes Nx = Nz of the plain workload (128: the headline configuration)")
     ap.add_argument("--serve-requests", type=int, default=30)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -32,7 +32,7 @@ def _rank(rank, world, port, out):
         times = bench.max_over_ranks([1.0 + rank, 5.0 - rank, 0.25 * rank], world, "cpu")
 
         class Args:
-            steps, warmup = 2, 3
+            steps, warmup, nx = 2, 3, 128
         buf = io.StringIO()
         if rank != 0:
             with redirect_stdout(buf):

@@ -238,14 +238,14 @@ def test_fast_and_generic_fft_paths_agree(N, monkeypatch):
         assert rel_l2(out[0][f], out[1][f]) <= (1e-12 if f == "p" else 1e-13), f
 
 
-@pytest.mark.parametrize("N,ctpress", [(16, 1), (32, 0), (64, 1), (128, 1)])
-def test_small_and_sequential_column_passes_agree(N, ctpress, monkeypatch):
+@pytest.mark.parametrize("N,ctpress,ny", [(16, 1, 97), (32, 0, 97), (64, 1, 97), (128, 1, 97), (32, 1, 257)])
+def test_small_and_sequential_column_passes_agree(N, ctpress, ny, monkeypatch):
     """The one-CTA-per-column pass (warp scans over the y rows) and the
     32-columns-per-CTA sequential pass give the same steps: only the values
     entering each lane's block of rows are formed in a different order.  Both
     are forced through LH_SMALL_COLUMNS, whichever the size would pick."""
     from lh_b200 import Desc, grids, perturbed_laminar
-    d = Desc(Nx=N, Nz=N, ny=97, flag_ctpress=ctpress, dt_mode=1, dt=1e-3)
+    d = Desc(Nx=N, Nz=N, ny=ny, flag_ctpress=ctpress, dt_mode=1, dt=1e-3)
     yu, yv = grids(d)
     ic = perturbed_laminar(d, 7, yu, yv)
     out = []
