@@ -108,3 +108,27 @@ def test_isolated_plans_equal_the_shared_plan(monkeypatch):
     for k in range(len(descs)):
         for f in ("u1", "u2", "u3", "p"):
             assert rel_l2(out[0][k][f], out[1][k][f]) <= 1e-14, (k, f)
+
+
+def test_batch_of_small_instances_uses_the_per_column_pass(monkeypatch):
+    """Plans of few columns run the one-CTA-per-column column pass, batches
+    included: two small instances in one batch give each instance's states
+    as it gives them alone (the per-column pass does not depend on the other
+    columns of the launch)."""
+    from lh_b200 import Batch, Desc, Engine
+    monkeypatch.setenv("LH_SMALL_COLUMNS", "1000000000")
+    descs = [Desc(Nx=16, Nz=16, ny=33, dt_mode=1, dt=1e-3), Desc(Nx=32, Nz=16, ny=65, dt_mode=0, CFL=0.5)]
+    ics = [_ic(d, 400 + k) for k, d in enumerate(descs)]
+    b = Batch()
+    slots = [b.add(d, *ic) for d, ic in zip(descs, ics)]
+    b.step(3)
+    b.synchronize()
+    for d, s, ic in zip(descs, slots, ics):
+        e = Engine(d)
+        e.upload(*ic)
+        e.step(3)
+        e.synchronize()
+        ref = e.download()
+        got = b.download(s)
+        for f in ("u1", "u2", "u3", "p"):
+            assert rel_l2(got[f], ref[f]) <= 1e-14, (d, f, rel_l2(got[f], ref[f]))
