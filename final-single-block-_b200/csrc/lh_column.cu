@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         const size_t o = (size_t)j * nc, on = o - nc;
                         cp16(ring.at(st, 0), U + o + nc);
                         cp16(ring.at(st, 1), P + on);
-                        cp16(ring.at(st, 2), N + on);
+                        if (kRK != 1) cp16(ring.at(st, 2), N + on);  // c_1 = 0: Nu_old unused
                         cp16(ring.at(st, 3), X + on);
                         cp16(ring.at(st, 4), FL + o);
                     },
@@ -237,7 +237,8 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                     [&](int r, const RowA &w) {
                         const int j = r + 1;
                         const size_t o = (size_t)j * nc, on = o - nc;
-                        const double2 up = w.a, pj = w.b, no = w.c, x = w.d, fl = w.e;
+                        const double2 up = w.a, pj = w.b, x = w.d, fl = w.e;
+                        const double2 no = kRK == 1 ? make_double2(0.0, 0.0) : w.c;
                         const double d1 = w.m0, d2 = w.m1, d3 = w.m2;
                         const double cen = k2x + k2z + d2;
                         const double2 L = make_double2(d1 * um.x + cen * uc.x + d3 * up.x, d1 * um.y + cen * uc.y + d3 * up.y);
@@ -284,7 +285,7 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         const size_t o = (size_t)j * nc, on = o - nc;
                         cp16(ring.at(st, 0), U2 + o + nc);
                         cp16(ring.at(st, 1), P + o);  // p(j+1)
-                        cp16(ring.at(st, 2), N + on);
+                        if (kRK != 1) cp16(ring.at(st, 2), N + on);  // c_1 = 0: Nu_old unused
                         cp16(ring.at(st, 3), X + on);
                         cp16(ring.at(st, 4), VV + o + nc);
                     },
@@ -296,7 +297,8 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                     [&](int r, const RowA &w) {
                         const int j = r + 1;
                         const size_t o = (size_t)j * nc, on = o - nc;
-                        const double2 up = w.a, pn = w.b, no = w.c, x = w.d, vvn = w.e;
+                        const double2 up = w.a, pn = w.b, x = w.d, vvn = w.e;
+                        const double2 no = kRK == 1 ? make_double2(0.0, 0.0) : w.c;
                         const double e1 = w.m0, e2 = w.m1, e3 = w.m2;
                         const double cenv = k2x + k2z + e2;
                         const double2 L = make_double2(e1 * um.x + cenv * uc.x + e3 * up.x, e1 * um.y + cenv * uc.y + e3 * up.y);
@@ -781,7 +783,8 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_column_small(const Inst *_
             const double2 um = O[j - 1], uc = O[j], up = O[j + 1];
             const size_t o = (size_t)j * nc, on = o - nc;
             // Nu_old is overwritten below in this iteration: a plain load
-            const double2 no = SN[on], x = __ldg(SX + on), fl = __ldg(FL + o), flp = __ldg(FL + on);
+            const double2 no = kRK == 1 ? z2 : SN[on];  // c_1 = 0: Nu_old unused at kRK = 1
+            const double2 x = __ldg(SX + on), fl = __ldg(FL + o), flp = __ldg(FL + on);
             const double2 pj = SP[j - 1];
             const double d1 = du[3 * j], d2 = du[3 * j + 1], d3 = du[3 * j + 2];
             const double cen = k2x + k2z + d2;
@@ -807,7 +810,8 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_column_small(const Inst *_
             const double2 um = O2[j - 1], uc = O2[j], up = O2[j + 1];
             const size_t o = (size_t)j * nc, on = o - nc;
             // Nu_old is overwritten below in this iteration: a plain load
-            const double2 no = SN2[on], x = __ldg(SX2 + on), vvc = __ldg(SVV + o), vvn = __ldg(SVV + o + nc);
+            const double2 no = kRK == 1 ? z2 : SN2[on];  // c_1 = 0: Nu_old unused at kRK = 1
+            const double2 x = __ldg(SX2 + on), vvc = __ldg(SVV + o), vvn = __ldg(SVV + o + nc);
             const double2 pc = SP[j - 1], pn = SP[j];
             const double e1 = dv[3 * j], e2 = dv[3 * j + 1], e3 = dv[3 * j + 2];
             const double cenv = k2x + k2z + e2;
