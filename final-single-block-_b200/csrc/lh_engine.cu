@@ -325,10 +325,14 @@ ClassTiles class_tiles(const HostSetup &s, bool force_generic)
     if (c.fast && ov && sscanf(ov, "%d,%d,%d", &a, &b, &d) == 3 && a > 0 && b > 0 && d > 0) return fast_tiles(s, a, b, d);
     if (c.fast) {
         // measured on B200 at 128^2 (16 threads per vector): 16 x modes per
-        // z-inverse CTA, 4 z rows per x CTA, up to 5 x modes per z-forward
-        // CTA; sizes with fewer threads per vector take proportionally more
+        // z-inverse CTA, 4 z rows per x CTA, up to 4 x modes per z-forward
+        // CTA; sizes with fewer threads per vector take proportionally more.
+        // The z-forward bound is 80/vz, one less at Mz = 96 and 192 (ny =
+        // 153 sweeps: one x mode fewer was faster there, slower at Mz = 288
+        // and 384, even at 48).
         const int vz = std::max(1, fast_vector_threads(s.Mz)), vx = std::max(1, fast_vector_threads(s.Mx));
-        c = fast_tiles(s, 256 / vz, std::max(1, 64 / vx), std::max(1, 80 / vz));
+        const int cbf = std::max(1, 80 / vz - ((s.Mz == 96 || s.Mz == 192) ? 1 : 0));
+        c = fast_tiles(s, 256 / vz, std::max(1, 64 / vx), cbf);
     } else {
         Tiles t = default_tiles(s.Mx, s.Mz, s.nxh, s.nyu);
         c.cbz = t.bc_zinv;
