@@ -1,13 +1,18 @@
 ! iso_c_binding bridge from the LittleHarsh Fortran driver to the B200
 ! engine (include/lh_gpu.h).  The Fortran main loop keeps its arrays and
-! its set-up; these wrappers forward them to the C ABI with the reference's
-! own subroutine names and argument lists, so littleharsh.f90 and FOU3D.f90
-! call sites stay as they are.  A non-zero status stops the run the way the
-! reference stops on bad input (start.f90:203-204).
+! its set-up.  This module holds the bind(C) interfaces, the context and the
+! whole-substep wrappers (gpu_*); lh_gpu_surface.f90 builds on it the
+! external subroutines with the reference's own names and argument lists
+! (four_to_phys_u, phys_to_four_du, LUsolU, LUsolP, LU_buildP, solveU,
+! solveP), so littleharsh.f90 and FOU3D.f90 call sites stay as they are.  A
+! non-zero status stops the run the way the reference stops on bad input
+! (start.f90:203-204).
 !
-! Build (Fortran compiler and the engine library required):
-!   mpif90 -c lh_gpu_bridge.f90
-!   mpif90 -o littleharsh <reference objects> lh_gpu_bridge.o \
+! Build (Fortran compiler and the engine library required; the declaration
+! module of the reference first):
+!   mpif90 -c declaration.f90 lh_gpu_bridge.f90 lh_gpu_surface.f90
+!   mpif90 -o littleharsh lh_gpu_surface.o lh_gpu_bridge.o <reference objects> \
+!          -Wl,--allow-multiple-definition \
 !          -L<repo>/final-single-block-_b200/build -llh_gpu -lcudart
 module lh_gpu_bridge
   use iso_c_binding
@@ -118,6 +123,41 @@ module lh_gpu_bridge
       integer(c_size_t), value :: cap
       integer(c_int)           :: count
     end function
+    integer(c_int) function lh_synchronize(ctx) bind(C, name="lh_synchronize")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function lh_error_div(ctx, err) bind(C, name="lh_error_div")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(out) :: err
+    end function
+    integer(c_int) function lh_tridiag_factor(ctx, grid, kRK, dt, a, cap) bind(C, name="lh_tridiag_factor")
+      import :: c_int, c_ptr, c_double, c_size_t
+      type(c_ptr), value       :: ctx
+      integer(c_int), value    :: grid, kRK
+      real(c_double), value    :: dt
+      real(c_double)           :: a(*)
+      integer(c_size_t), value :: cap
+    end function
+    integer(c_int) function lh_tridiag_solve(ctx, grid, a, x) bind(C, name="lh_tridiag_solve")
+      import :: c_int, c_ptr, c_double, c_double_complex
+      type(c_ptr), value    :: ctx
+      integer(c_int), value :: grid
+      real(c_double), intent(in) :: a(*)
+      complex(c_double_complex)  :: x(*)
+    end function
+    integer(c_int) function lh_set_dg(ctx, a) bind(C, name="lh_set_dg")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: a(*)
+    end function
+    integer(c_int) function lh_set_scalars(ctx, t, iter, mpgx) bind(C, name="lh_set_scalars")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value    :: ctx
+      real(c_double), value :: t, mpgx
+      integer(c_int), value :: iter
+    end function
   end interface
 
   type(c_ptr), save :: gpu_ctx = c_null_ptr
@@ -145,10 +185,48 @@ contains
     call gpu_check(lh_ctx_create(d, gpu_ctx), 'lh_ctx_create')
   end subroutine
 
-  ! After getini(): hand the initial state to the device.
+  ! The context, created from the declaration module on first use by the
+  ! reference-named routines of lh_gpu_surface.f90.
+  subroutine gpu_ensure()
+    if (.not. c_associated(gpu_ctx)) call gpu_start()
+  end subroutine
+
+  ! Column count and row counts of the declaration module (np = 1).
+  integer(c_size_t) function gpu_cols()
+    use declaration, only: columns_num
+    gpu_cols = int(columns_num(0), c_size_t)
+  end function
+
+  ! After getini(): hand the initial state to the device, with the t, iter
+  ! and mpgx getini left in the declaration module (zero / the input deck's
+  ! for flag_init = 1, the restart file's for flag_init = 2,
+  ! start.f90:1268-1282).
   subroutine gpu_getini(u1, u2, u3, p)
+    use declaration, only: t, iter, mpgx
     complex(8), intent(in) :: u1(*), u2(*), u3(*), p(*)
     call gpu_check(lh_upload_state(gpu_ctx, u1, u2, u3, p), 'lh_upload_state')
+    call gpu_check(lh_set_scalars(gpu_ctx, t, int(iter, c_int), mpgx), 'lh_set_scalars')
+  end subroutine
+
+  ! Refresh the declaration module's t, dt, iter, mpgx and Qx from the
+  ! device (the main loop's do while (t < maxt) test, hist output).
+  subroutine gpu_scalars()
+    use declaration, only: t, dt, iter, mpgx, Qx
+    integer(c_int) :: it
+    call gpu_check(lh_get_scalars(gpu_ctx, t, dt, it, mpgx, Qx), 'lh_get_scalars')
+    iter = it
+  end subroutine
+
+  ! error(div) (littleharsh.f90:370-409): max |div| of the current state
+  subroutine gpu_error(err_out)
+    real(8), intent(out) :: err_out
+    call gpu_check(lh_error_div(gpu_ctx, err_out), 'lh_error_div')
+  end subroutine
+
+  ! The engine uses the caller's DG (start.f90:636) as its pressure factors.
+  subroutine gpu_set_dg(DG_in)
+    real(8), intent(in) :: DG_in(*)
+    call gpu_check(lh_set_dg(gpu_ctx, DG_in), 'lh_set_dg')
   end subroutine
 
   ! Replaces the body of the substep loop, littleharsh.f90:169-220
@@ -164,33 +242,6 @@ contains
     call gpu_check(lh_download_state(gpu_ctx, u1, u2, u3, p), 'lh_download_state')
   end subroutine
 
-  ! four_to_phys_u / phys_to_four_du on one plane (FOU3D.f90:653, 1654)
-  subroutine gpu_four_to_phys_du(du)
-    real(8) :: du(*)
-    call gpu_check(lh_four_to_phys(gpu_ctx, du, 1_c_int), 'lh_four_to_phys')
-  end subroutine
-
-  subroutine gpu_phys_to_four_du(duPL)
-    real(8) :: duPL(*)
-    call gpu_check(lh_phys_to_four(gpu_ctx, duPL, 1_c_int), 'lh_phys_to_four')
-  end subroutine
-
-  ! LUsolU(u, rhsu, a, grid, myid) without the a(3,:) work array
-  ! (tridLU_3D.f90:38-94); uses the module's kRK and dt.
-  subroutine gpu_LUsolU(u, rhsu, grid)
-    use declaration, only: kRK, dt
-    complex(8), intent(out) :: u(*)
-    complex(8), intent(in)  :: rhsu(*)
-    integer, intent(in)     :: grid
-    call gpu_check(lh_lusolu(gpu_ctx, int(grid, c_int), int(kRK, c_int), dt, rhsu, u), 'lh_lusolu')
-  end subroutine
-
-  ! LUsolP(x, myid, nystart, nyend) with the DG factors of start()
-  subroutine gpu_LUsolP(x)
-    complex(8) :: x(*)
-    call gpu_check(lh_lusolp(gpu_ctx, x), 'lh_lusolp')
-  end subroutine
-
   ! spectra(u1,u2,u2_itp,u3,p,myid) at a flagged step (FOU3D.f90:137-141):
   ! the accumulation stays on the device
   subroutine gpu_spectra()
@@ -198,14 +249,26 @@ contains
   end subroutine
 
   ! Bring the accumulated spectra back before write_spect (spectra.f90)
+  ! The capacities are the sizes of spU/spW/spUV (jlim(:,ugrid) rows), spV
+  ! (vgrid rows) and spP (pgrid rows) times the columns (start.f90:641-645).
   subroutine gpu_fetch_spectra(spU_, spV_, spW_, spUV_, spP_)
+    use declaration, only: nyu, nyv
     real(8) :: spU_(*), spV_(*), spW_(*), spUV_(*), spP_(*)
-    integer(c_int) :: n
-    n = lh_get_spectra(gpu_ctx, 0_c_int, spU_, huge(0_c_size_t), n)
-    n = lh_get_spectra(gpu_ctx, 1_c_int, spV_, huge(0_c_size_t), n)
-    n = lh_get_spectra(gpu_ctx, 2_c_int, spW_, huge(0_c_size_t), n)
-    n = lh_get_spectra(gpu_ctx, 3_c_int, spUV_, huge(0_c_size_t), n)
-    n = lh_get_spectra(gpu_ctx, 4_c_int, spP_, huge(0_c_size_t), n)
+    integer(c_int) :: n, cnt
+    integer(c_size_t) :: cu, cv, cp
+    cu = int(nyu + 2, c_size_t) * gpu_cols()
+    cv = int(nyv + 2, c_size_t) * gpu_cols()
+    cp = int(nyu, c_size_t) * gpu_cols()
+    n = lh_get_spectra(gpu_ctx, 0_c_int, spU_, cu, cnt)
+    if (n < 0) call gpu_check(n, 'lh_get_spectra')
+    n = lh_get_spectra(gpu_ctx, 1_c_int, spV_, cv, cnt)
+    if (n < 0) call gpu_check(n, 'lh_get_spectra')
+    n = lh_get_spectra(gpu_ctx, 2_c_int, spW_, cu, cnt)
+    if (n < 0) call gpu_check(n, 'lh_get_spectra')
+    n = lh_get_spectra(gpu_ctx, 3_c_int, spUV_, cu, cnt)
+    if (n < 0) call gpu_check(n, 'lh_get_spectra')
+    n = lh_get_spectra(gpu_ctx, 4_c_int, spP_, cp, cnt)
+    if (n < 0) call gpu_check(n, 'lh_get_spectra')
   end subroutine
 
   ! stats(myid,status,ierr) at the flagst steps (FOU3D.f90:307-341), with
@@ -222,18 +285,21 @@ contains
   ! The plane sums acc(0:nyu+1, 13) = Um U2m Vm V2m Wm W2m UVm UWm VWm Pm P2m
   ! wxm wx2m, with the number of accumulations (istat)
   subroutine gpu_fetch_stats(acc, nstat_done)
+    use declaration, only: nyu
     real(8) :: acc(*)
     integer :: nstat_done
     integer(c_int) :: n, cnt
-    n = lh_get_stats(gpu_ctx, acc, huge(0_c_size_t), cnt)
+    n = lh_get_stats(gpu_ctx, acc, 13_c_size_t * int(nyu + 2, c_size_t), cnt)
+    if (n < 0) call gpu_check(n, 'lh_get_stats')
     nstat_done = cnt
   end subroutine
 
   ! omega_x at the v faces, wx(Nspec_x+2, Nspec_z, 0:nyu+1) in physical space
-  subroutine gpu_omega_x(wx)
-    real(8) :: wx(*)
+  subroutine gpu_omega_x(wx_out)
+    use declaration, only: nyu, Nspec_x, Nspec_z
+    real(8) :: wx_out(*)
     integer(c_int) :: n
-    n = lh_omega_x(gpu_ctx, wx, huge(0_c_size_t))
+    n = lh_omega_x(gpu_ctx, wx_out, int(nyu + 2, c_size_t) * int(Nspec_z, c_size_t) * int(Nspec_x + 2, c_size_t))
     if (n < 0) call gpu_check(n, 'lh_omega_x')
   end subroutine
 

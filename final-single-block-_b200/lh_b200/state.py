@@ -185,8 +185,11 @@ def read_state(dirin: str, tag: str, desc: Desc, np1: bool = True):
 
 
 def write_state(dirout: str, tag: str, desc: Desc, u1, u2, u3, p, yu, yv, dthdyu, dthdyv,
-                t: float = 0.0, it: int = 0) -> None:
-    """Write the four spectral files the way record_out does (FOU3D.f90:2063-2165)."""
+                t: float = 0.0, it: int = 0, mpgx: float | None = None) -> None:
+    """Write the four spectral files the way record_out does (FOU3D.f90:2063-2165).
+    The header carries t, iter and the current mpgx (which the constant flow
+    rate mode changes; default: the description's)."""
+    mp = desc.mpgx if mpgx is None else float(mpgx)
     N = np.zeros((4, 5), np.int32)
     N[0, 1:4] = desc.Nx
     N[0, 4] = -2
@@ -196,7 +199,7 @@ def write_state(dirout: str, tag: str, desc: Desc, u1, u2, u3, p, yu, yv, dthdyu
     for name, arr, lo, y, dth, ident in (("u1", u1, 0, yu, dthdyu, 1), ("u2", u2, 0, yv, dthdyv, 2),
                                          ("u3", u3, 0, yu, dthdyu, 3), ("p", p, 1, yu, dthdyu, 4)):
         with open(os.path.join(dirout, name + tag), "wb") as f:
-            h = struct.pack("<5d", t, desc.Re, desc.alp, desc.bet, desc.mpgx) + struct.pack("<2i", 3, it)
+            h = struct.pack("<5d", t, desc.Re, desc.alp, desc.bet, mp) + struct.pack("<2i", 3, it)
             h += np.zeros(88, np.int32).tobytes()
             f.write(_rec(h))
             f.write(_rec(N.T.astype("<i4").tobytes()))

@@ -109,6 +109,22 @@ int lh_step_host(lh_ctx *ctx, double *u1, double *u2, double *u3, double *p,
 int lh_synchronize(lh_ctx *ctx);
 /* The CUDA stream (cudaStream_t) every call of this context is ordered on. */
 int lh_get_stream(lh_ctx *ctx, void **stream);
+/* Autotuner of the launch shapes (no counterpart in the reference, whose
+ * shapes are fixed by FFTPACK's factorisation, cft_buff.f:141-163,
+ * rft_buff.f:133-160): the plane pipeline's tile bounds (x modes per
+ * z-inverse CTA, z rows per x-products CTA, x modes per z-forward CTA), the
+ * plane-staging budget and the number of column-pass launches for this
+ * context's size, chosen by timing RK3 steps of a scratch instance (the
+ * context's state is not touched; its current state is copied in so the CFL
+ * step is the run's).  None of them changes any arithmetic: the states stay
+ * bit-identical.  Results are cached per GPU name and (Mz, Mx, nyu) in the
+ * file LH_TUNE_CACHE (default lh_tune_cache.txt beside the library) and in a
+ * process-wide table that every later plan of that size -- contexts and
+ * batches -- uses.  force = 1 measures even when the cache has the size.
+ * params (may be NULL) receives [cbz, rbx, cbf, staging_mb, col_waves,
+ * source], source 1 = measured now, 2 = read from the cache.  Allocates one
+ * scratch instance for the duration of the call. */
+int lh_autotune(lh_ctx *ctx, int force, int *params);
 /* Runs nsteps RK3 steps launch by launch with CUDA events around every
  * kernel and returns, per kernel class (0 z-inverse, 1 x-products,
  * 2 z-forward, 3 dt, 4 column), the summed milliseconds and launch counts. */
@@ -183,6 +199,36 @@ int lh_phys_to_four(lh_ctx *ctx, double *planes, int nplanes);
 int lh_lusolu(lh_ctx *ctx, int grid, int kRK, double dt, const double *rhs,
               double *u);
 int lh_lusolp(lh_ctx *ctx, double *x);
+
+/* ---- tridiagonal factors in the reference's a(3, j, column) layout -----
+ * (tridLU_3D.f90): a(1,j) lower diagonal, a(2,j) inverse pivot, a(3,j)
+ * scaled upper diagonal, j from jlim(1,grid), 3 doubles per row, rows
+ * fastest within a column.  grid: 2 = u/w (j = 0..nyu+1), 1 = v (j =
+ * 0..nyv+1), 3 = p (j = 1..nyu).
+ *
+ * lh_tridiag_factor replaces LU_build + LU_dec (tridLU_3D.f90:163-221,
+ * 327-364) of every column for RK substep kRK and time step dt (grid 1, 2;
+ * computed on the device with the reference's operation order), and, for
+ * grid = 3, returns the pressure factors DG of LU_buildP + LU_decP
+ * (tridLU_3D.f90:224-297, 366-407; start.f90:636) the engine uses (kRK, dt
+ * ignored).  Returns the double count 3 x rows x ncols; a = NULL only
+ * queries it, cap is the capacity of a in doubles.
+ * lh_tridiag_solve replaces the solve of LUsolU / LUsolP with factors the
+ * caller holds (tridLU_3D.f90:70-82, 115-128): x is x(j, column), complex,
+ * solved in place.
+ * lh_set_dg installs a caller's DG (the start.f90:636 array, grid 3 layout)
+ * as the engine's pressure factors; its lower diagonal a(1,j) must be the
+ * same in every column, as LU_buildP forms it (LH_EINVAL otherwise). */
+int lh_tridiag_factor(lh_ctx *ctx, int grid, int kRK, double dt, double *a, size_t cap);
+int lh_tridiag_solve(lh_ctx *ctx, int grid, const double *a, double *x);
+int lh_set_dg(lh_ctx *ctx, const double *a);
+
+/* ---- continuing a run: getini with flag_init = 2 (start.f90:1268-1282)
+ * takes t and iter from the restart file's header and keeps its mpgx.  Call
+ * after lh_upload_state (which starts t and iter at 0 and mpgx at the
+ * description's); the state must be the complete one (read_in at one rank
+ * leaves the top ghost plane of u1/u3 at zero, which changes the next step). */
+int lh_set_scalars(lh_ctx *ctx, double t, int iter, double mpgx);
 
 /* Allocation-free LUsolU for callers that cannot allocate device memory
  * per call (inside CUDA-graph capture, in a loop that must not hit the

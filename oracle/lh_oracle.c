@@ -1051,6 +1051,13 @@ static void lusolu(lho_ctx *c, int grid, int kRK, const double *rhs, double *u)
 
 void lho_lusolu(lho_ctx *c, int grid, int kRK, const double *rhs, double *u) { lusolu(c, grid, kRK, rhs, u); }
 
+/* LU_build + LU_dec of every column of a velocity grid, a(3, j, column) */
+void lho_lu_factor(const lho_ctx *c, int grid, int kRK, double *a)
+{
+    int len = grid == UGRID ? c->nyu + 2 : c->nyv + 2;
+    for (int col = 1; col <= c->ncols; col++) lu_build_dec(c, grid, col, kRK, a + (size_t)3 * len * (col - 1));
+}
+
 /* LUsolP (tridLU_3D.f90:98-132) */
 void lho_lusolp(const lho_ctx *c, double *x)
 {

@@ -116,6 +116,9 @@ void lho_der_z(const lho_ctx *c, const double *u, double *dudz);
 /* LUsolU on every column for one grid (tridLU_3D.f90:38-94); grid 2 = u, 1 = v.
  * rhs and u in column layout; uses current dt and kRK. */
 void lho_lusolu(lho_ctx *c, int grid, int kRK, const double *rhs, double *u);
+/* LU_build + LU_dec (tridLU_3D.f90:163-221, 327-364) of every column of grid
+ * (2 u/w, 1 v) at RK substep kRK with the context's dt: a(3, j, column) */
+void lho_lu_factor(const lho_ctx *c, int grid, int kRK, double *a);
 /* LUsolP on every column (tridLU_3D.f90:98-132), in place */
 void lho_lusolp(const lho_ctx *c, double *x);
 

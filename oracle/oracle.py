@@ -83,6 +83,7 @@ def lib(threaded: bool = False) -> ctypes.CDLL:
     L.lho_der_z.argtypes = [v, dp, dp]
     L.lho_lusolu.argtypes = [v, i, i, dp, dp]
     L.lho_lusolp.argtypes = [v, dp]
+    L.lho_lu_factor.argtypes = [v, i, i, dp]
     L.lho_error_div.restype = d
     L.lho_error_div.argtypes = [v]
     L.lho_spectra.argtypes = [v, dp, dp, dp, dp, dp]

@@ -11,6 +11,11 @@ stores, as compressed numpy archives:
   u1/u3 planes 0..nyu, u2 planes 0..nyv+1, p planes 1..nyu, complex per
   column [column, j]; the top ghost plane of u1/u3 is left zero as read_in
   leaves it.  Header scalars t, Re, alp, bet, mpgx, iter are kept too.
+* ``ref_turb_0128x0128x0153.npz`` -- the same for the reference's developed
+  turbulent 128x128x153 field at t = 945.5 (``*_0128x0128x0153_t09455.dat``).
+  At ~81 MB it is not committed (``.gitignore`` lists it): this script makes
+  it in a checkout that has the reference tree beside it, and the test that
+  steps it skips, naming this script, where the file is absent.
 
 Usage:  python tests/golden/make_golden.py /path/to/reference
 """
@@ -36,9 +41,13 @@ def main(ref: str) -> None:
     np.savez_compressed(os.path.join(HERE, "ref_ic_0032x0032x0153.npz"),
                         u1=u1, u2=u2, u3=u3, p=p,
                         t=f1.t, Re=f1.Re, alp=f1.alp, bet=f1.bet, mpgx=f1.mpgx, iter=f1.iter)
-    # the 128x128 case shares the grid; keep only its header check values
+    # the 128x128 turbulent field shares the grid
     f128 = O.read_dat(os.path.join(inp, "u1_0128x0128x0153_t09455.dat"))
     assert np.array_equal(f128.y, fu.y)
+    u1, u2, u3, p, f1 = O.read_in_np1(inp, "_0128x0128x0153_t09455.dat", 128, 128, nyu, nyv)
+    np.savez(os.path.join(HERE, "ref_turb_0128x0128x0153.npz"),
+             u1=u1, u2=u2, u3=u3, p=p,
+             t=f1.t, Re=f1.Re, alp=f1.alp, bet=f1.bet, mpgx=f1.mpgx, iter=f1.iter)
     print("wrote golden fixtures to", HERE)
 
 

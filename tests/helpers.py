@@ -30,3 +30,14 @@ def oracle_cfg(desc, threaded=False) -> "O.Config":
 def golden_ic():
     z = np.load(os.path.join(GOLDEN, "ref_ic_0032x0032x0153.npz"))
     return z["u1"], z["u2"], z["u3"], z["p"]
+
+
+# Per-field errors of every parity case of a run, in the order the cases ran;
+# written out by the session hook in conftest.py when LH_PARITY_OUT names a
+# file (a JSON list of {"case", "bar", "errors"}).
+PARITY_RECORD: list = []
+
+
+def record(case: str, errs: dict, bar: float) -> None:
+    PARITY_RECORD.append({"case": case, "bar": bar, "errors": {k: float(v) for k, v in errs.items()}})
+    print(case, {k: f"{v:.2e}" for k, v in errs.items()})
