@@ -174,12 +174,12 @@ def cpu_rate(desc, sample_steps: int, threads: int):
     """Reference algorithm on the host (oracle, OpenMP) -> (rate, seconds, cores)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    from lh_b200 import grids, perturbed_laminar
+    from lh_b200.state import perturbed_laminar  # numpy only: the engine library is not loaded
     cfg = O.Config(Nx=desc.Nx, Nz=desc.Nz, ny=desc.ny, Re=desc.Re, mpgx=desc.mpgx, dt_mode=O.DT_FIXED,
                    dt_fixed=desc.dt, nthreads=threads)
-    yu, yv = grids(desc)
-    ic = perturbed_laminar(desc, 20260002, yu, yv)
     o = O.Oracle(cfg, threaded=True)
+    yu, yv = o.array(0), o.array(1)  # the oracle's own ygrid
+    ic = perturbed_laminar(desc, 20260002, yu, yv)
     o.load_state(*ic)
     o.step(1)  # warm caches and page in
     t0 = time.perf_counter()
@@ -232,10 +232,23 @@ def substep_alg_bytes(desc):
 DESIGN_F = {"z_inverse": 3, "x_products": 0, "z_forward": 6, "dt": 0, "column": 20}
 
 
+def _batch_rate(b, pts, K):
+    """grid-pt*substeps/s of a batch over K timed steps (after 3 warm steps)."""
+    b.step(3)
+    b.synchronize()
+    t0 = time.perf_counter()
+    b.step(K)
+    b.synchronize()
+    bt = time.perf_counter() - t0
+    return pts * 3 * K / bt, 1e3 * bt / K
+
+
 def batched_and_served(args):
-    """Throughput of the batched engine (64 instances of 32x32x153, Re_tau and
-    dt drawn per instance) and of the serving loop on a scaled Poisson stream,
-    next to the plain single-instance path on the same stream."""
+    """Throughput of the batched engine on the uniform batch (64 instances of
+    32x32x153, Re_tau and dt drawn per instance) and on the uneven batch (16 x
+    32^2, 8 x 64^2, 4 x 128^2 at ny = 153 and 1 x 256^2 x 257, Re_tau in
+    [180, 550], tanh(2) grid), and of the serving loop on a Poisson stream,
+    next to the plain single-instance path on the same stream and clock."""
     from lh_b200 import Batch, Desc, grids, perturbed_laminar, re_from_retau
     from lh_b200.serve import poisson_stream, run_plain, serve
     rng = np.random.default_rng(20260003)
@@ -247,31 +260,50 @@ def batched_and_served(args):
         yu, yv = grids(d)
         b.add(d, *perturbed_laminar(d, 20260003 + 1000 * k, yu, yv))
         pts += d.points()
-    b.step(3)
-    b.synchronize()
-    K = 10
-    t0 = time.perf_counter()
-    b.step(K)
-    b.synchronize()
-    bt = time.perf_counter() - t0
+    rate, ms = _batch_rate(b, pts, 10)
     b.close()
     batched = {"workload": "64 instances of 32x32x153, Re_tau~U[100,400], dt~U[5e-4,2e-3], one launch per "
                            "kernel class and chunk round per substep, CUDA graph",
-               "value": pts * 3 * K / bt, "unit": UNIT, "ms_per_step": 1e3 * bt / K}
+               "value": rate, "unit": UNIT, "ms_per_step": ms}
+    rng = np.random.default_rng(20260004)
+    b = Batch()
+    pts = 0
+    k = 0
+    for n, ny, count in ((32, 153, 16), (64, 153, 8), (128, 153, 4), (256, 257, 1)):
+        for _ in range(count):
+            d = Desc(Nx=n, Nz=n, ny=ny, Re=re_from_retau(rng.uniform(180, 550), MPGX), mpgx=MPGX, grid_type=1,
+                     gamma=2.0, dt_mode=1, dt=2.5e-4 if n >= 128 else 5e-4)
+            yu, yv = grids(d)
+            b.add(d, *perturbed_laminar(d, 20260004 + 1000 * k, yu, yv))
+            pts += d.points()
+            k += 1
+    rate_u, ms_u = _batch_rate(b, pts, 10)
+    b.close()
+    uneven = {"workload": "16 x 32x32x153, 8 x 64x64x153, 4 x 128x128x153 and 1 x 256x256x257, Re_tau~U[180,550], "
+                          "tanh(2) y grid, dt 5e-4 (2.5e-4 at 128^2 and above), shared substep launches, CUDA graph; "
+                          "10 timed steps (the configuration's 500-step run measured on a sample)",
+              "value": rate_u, "unit": UNIT, "ms_per_step": ms_u}
     n_req = args.serve_requests
+    steps = (200, 5000) if args.serve_full_steps else (20, 200)
+    scale = args.serve_time_scale
     mk = lambda: poisson_stream(n_req, 4.0, np.random.default_rng(20260005), [32, 64, 128, 192], [97, 153, 257],
-                                steps=(20, 200))
+                                steps=steps)
     reqs = mk()
-    st = serve(reqs, hbm_budget=150 << 30, max_chunk=50, keep_results=False, time_scale=0.25)
+    st = serve(reqs, hbm_budget=150 << 30, max_chunk=50, keep_results=False, time_scale=scale)
     reqs2 = mk()
-    tp = run_plain(reqs2, keep_results=False)
-    served = {"workload": f"{n_req} requests, Poisson arrivals (4/s, replayed 4x faster), grids "
-                          "{32,64,128,192}^2 x ny {97,153,257}, Re_tau~U[100,550], steps log-U[20,200] "
-                          "(the serving config with 25x shorter requests), 150 GB budget",
+    tp = run_plain(reqs2, keep_results=False, time_scale=scale)
+    work = sum(r.work for r in reqs2)
+    ttc_plain = [r.finished - r.arrival * scale for r in reqs2]
+    served = {"workload": f"{n_req} requests, Poisson arrivals (4/s, replayed at {scale:g}x the arrival times), "
+                          f"grids {{32,64,128,192}}^2 x ny {{97,153,257}}, Re_tau~U[100,550], steps "
+                          f"log-U[{steps[0]},{steps[1]}], 150 GB budget",
               "value": st.throughput, "unit": UNIT, "p50_ttc_s": st.p50, "p99_ttc_s": st.p99,
               "mean_live": st.mean_live, "max_live": st.max_live, "wall_s": st.wall,
-              "plain_same_stream": sum(r.work for r in reqs2) / tp}
-    return batched, served
+              "plain_same_stream": work / tp, "plain_wall_s": tp,
+              "plain_p50_ttc_s": float(np.percentile(ttc_plain, 50)),
+              "plain_p99_ttc_s": float(np.percentile(ttc_plain, 99)),
+              "served_over_plain": st.throughput / (work / tp)}
+    return batched, uneven, served
 
 
 def max_over_ranks(vals, world, device):
@@ -371,9 +403,9 @@ def run_ours(args, rank, world, local_rank):
     (e2e_ms,) = max_over_ranks([ev2.elapsed_time(ev3)], world, "cuda")
     e2e_val = job_rate(world, pts_sub * Ke, e2e_ms * 1e-3)
 
-    batched = served = None
+    batched = uneven = served = None
     if rank == 0 and world == 1 and not args.no_serve:
-        batched, served = batched_and_served(args)
+        batched, uneven, served = batched_and_served(args)
 
     fp64 = None
     if rank == 0 and world == 1:
@@ -408,6 +440,7 @@ def run_ours(args, rank, world, local_rank):
             "dominant_kernel": dom[0],
             "cpu_baseline": cpu,
             "batched": batched,
+            "batched_uneven": uneven,
             "served": served,
             "clocks": clk.summary(),
         }
@@ -426,6 +459,10 @@ def main():
     ap.add_argument("--nx", type=int, default=128,
                     help="Fourier modes Nx = Nz of the plain workload (128: the headline configuration)")
     ap.add_argument("--serve-requests", type=int, default=30)
+    ap.add_argument("--serve-full-steps", action="store_true",
+                    help="served stream with the configuration's step counts log-U[200,5000] (default 20..200)")
+    ap.add_argument("--serve-time-scale", type=float, default=0.25,
+                    help="arrival times are replayed at this factor (<1: compressed)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -37,6 +37,7 @@ struct lh_batch {
     Inst *d_insts = nullptr;
     size_t d_insts_cap = 0;
     cudaStream_t st = nullptr;
+    cudaStream_t st_up = nullptr;  // admissions upload here while steps run on st
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     bool dirty = true;
@@ -104,6 +105,11 @@ extern "C" int lh_batch_create(size_t budget, lh_batch **out)
         delete b;
         return LH_ECUDA;
     }
+    if (cudaStreamCreateWithFlags(&b->st_up, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamDestroy(b->st);
+        delete b;
+        return LH_ECUDA;
+    }
     *out = b;
     return LH_OK;
 }
@@ -118,6 +124,7 @@ extern "C" int lh_batch_destroy(lh_batch *b)
     for (auto &s : b->slots)
         if (s) instance_free(*s);
     pool_release(b, 0);
+    if (b->st_up) cudaStreamDestroy(b->st_up);
     if (b->st) cudaStreamDestroy(b->st);
     delete b;
     return LH_OK;
@@ -147,8 +154,11 @@ extern "C" int lh_batch_add(lh_batch *b, const lh_grid_desc *desc, const double 
     const size_t need = instance_bytes(d->hs, t.chunk);
     if (b->budget && b->used + need > b->budget)
         return bfail(b, LH_ENOMEM, "HBM budget exhausted");
-    // instances are admitted between steps; wait for in-flight work first
-    BCK(cudaStreamSynchronize(b->st), "synchronize");
+    // The new instance is allocated and uploaded on the admission stream
+    // while steps already queued on the batch stream keep running: its memory
+    // is fresh or a pooled block of an instance retired after a
+    // synchronisation (lh_batch_remove), so no queued step touches it, and the
+    // next lh_batch_step synchronises before it rebuilds the step graph.
     // smallest pooled block that fits; else make room under the budget and allocate
     int pick = -1;
     for (size_t k = 0; k < b->pool.size(); k++)
@@ -163,13 +173,13 @@ extern "C" int lh_batch_add(lh_batch *b, const lh_grid_desc *desc, const double 
     } else if (b->budget) {
         pool_release(b, b->budget > b->used + need ? b->budget - b->used - need : 0);
     }
-    cudaError_t e = instance_alloc(*d, t.chunk, b->st, reuse, reuse_bytes);
+    cudaError_t e = instance_alloc(*d, t.chunk, b->st_up, reuse, reuse_bytes);
     if (e == cudaErrorMemoryAllocation && !reuse && !b->pool.empty()) {
         cudaGetLastError();
         pool_release(b, 0);
-        e = instance_alloc(*d, t.chunk, b->st);
+        e = instance_alloc(*d, t.chunk, b->st_up);
     }
-    if (e == cudaSuccess) e = instance_upload(*d, u1, u2, u3, p, b->st);
+    if (e == cudaSuccess) e = instance_upload(*d, u1, u2, u3, p, b->st_up);
     if (e != cudaSuccess) {
         instance_free(*d);
         return bcuda(b, e, "admit");
@@ -213,6 +223,9 @@ extern "C" int lh_batch_remove(lh_batch *b, int slot)
 static int rebuild(lh_batch *b)
 {
     if (!b->dirty) return LH_OK;
+    // queued steps still read the work tables and the instance table that
+    // are rewritten below
+    BCK(cudaStreamSynchronize(b->st), "synchronize");
     drop_graph(b);
     b->live.clear();
     b->any_cfl = false;

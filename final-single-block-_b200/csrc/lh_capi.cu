@@ -52,7 +52,8 @@ extern "C" int lh_ctx_create(const lh_grid_desc *desc, lh_ctx **out)
         delete c;
         return LH_ECUDA;
     }
-    cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    cudaError_t e = cudaGetDevice(&c->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete c;
         return LH_ECUDA;

@@ -16,13 +16,15 @@
 //            only, littleharsh.f90:515-548), divergence and the Poisson
 //            right-hand side (:645-658), LUsolP forward sweep with the set-up
 //            DG factors (tridLU_3D.f90:118-124).
-//   D1 (down, u1 warp)  LUsolP back sweep and p += psi.
-//   D2 (up, all warps)  v_corr and the ghost rows (littleharsh.f90:896-993).
+//   D (down, u1 warp)   LUsolP back sweep, p += psi and v_corr with the ghost
+//            rows (littleharsh.f90:896-993) in one sweep: row j of psi is
+//            final when the sweep reaches it, and u1, u3 need psi(j), u2
+//            psi(j) and psi(j+1), so each row of the state is written once.
 //
 // Block barriers separate the phases; every lane reaches them, columns past
 // the instance's last only skip the work.  Intermediate y rows are written
 // in place into the state arrays; the scaled upper diagonals go to FACU/FACV
-// for the back substitution.
+// for the back substitution, the forward sweep of LUsolP to PSI.
 #include "lh_kernels.cuh"
 
 namespace lh {
@@ -151,12 +153,8 @@ struct RowC {
     double g2, th, g1;
 };
 struct RowD {
-    double2 x, p;
-    double g3;
-};
-struct RowE {
-    double2 a, ps;
-    double th;
+    double2 x, p, u1, u3, u2;
+    double g3, th;
 };
 
 __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__restrict__ insts,
@@ -195,9 +193,9 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
     const double *du = sdu, *dv = sdv;
     double2 *warp_mem = ring_mem + (size_t)role * kWarpSlots * kColThreads;
     using RingA = Ring<kWarpSlots / 5, 5>;         // phase A: 5 slots per row
-    using RingW2 = Ring<kWarpSlots / 2, 2>;        // phases B, D2: 2 slots per row
+    using RingW2 = Ring<kWarpSlots / 2, 2>;        // phase B: 2 slots per row
     using RingC = Ring<kRoles * kWarpSlots / 4, 4>;   // phase C (u1 warp, all slots)
-    using RingD = Ring<kRoles * kWarpSlots / 3, 3>;   // phase D1 (u1 warp, all slots)
+    using RingD = Ring<kRoles * kWarpSlots / 6, 6>;   // phase D (u1 warp, all slots)
 
     // ---------------- A: right-hand sides and forward elimination --------
     if (live && role < 2) {
@@ -440,65 +438,68 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         PS[(size_t)(j - 1) * nc] = xp;
                         v2m = v2c;
                     });
-        // ---------------- D1: LUsolP back sweep and p += psi ---------------
+        // ---------------- D: LUsolP back sweep, p += psi and v_corr ---------
+        // One downward sweep of the u1 warp (tridLU_3D.f90:125-127,
+        // littleharsh.f90:660-664, v_corr :896-993): psi(j) from the forward
+        // sweep's x(j), then row j of p, u1 and u3, and row j of u2 with
+        // psi(j+1) of the previous row; psi itself is never stored.
         const double *G3 = I.DG3 + cc;
+        const double dtrk = dt * (rk.a + rk.b);
+        const double kd1 = dtrk * kxr, kd3 = dtrk * kzr, dtrk_u2 = dtrk * ddv;
         double2 psn = xp;  // psi(nyu) = x(nyu)
+        double2 first1 = make_double2(0.0, 0.0), first3 = first1, last1 = first1, last3 = first1, ps1 = first1;
         const RingD ringd{ring_mem, lane};
         stream_rows<RingD::kDepth, 4>(nyu,
                     [&](int r, int st) {
                         const int j = nyu - r;
-                        const size_t o = (size_t)(j - 1) * nc;
+                        const size_t o = (size_t)(j - 1) * nc, oj = (size_t)j * nc;
                         cp16(ringd.at(st, 0), PS + o);
                         cp16(ringd.at(st, 1), P + o);
                         if (j < nyu) cp8(&ringd.at(st, 2)->x, G3 + o);
+                        cp16(ringd.at(st, 3), U1 + oj);
+                        cp16(ringd.at(st, 4), U3 + oj);
+                        if (j <= nyv) cp16(ringd.at(st, 5), U2 + oj);
                     },
                     [&](int r, int st) {
                         const int j = nyu - r;
-                        return RowD{*ringd.at(st, 0), *ringd.at(st, 1), j < nyu ? ringd.at(st, 2)->x : 0.0};
+                        return RowD{*ringd.at(st, 0), *ringd.at(st, 1), *ringd.at(st, 3), *ringd.at(st, 4),
+                                    *ringd.at(st, 5), j < nyu ? ringd.at(st, 2)->x : 0.0, sthv[j]};
                     },
                     [&](int r, const RowD &w) {
                         const int j = nyu - r;
-                        const size_t o = (size_t)(j - 1) * nc;
+                        const size_t o = (size_t)(j - 1) * nc, oj = (size_t)j * nc;
                         double2 ps = w.x;
                         if (j < nyu) ps = make_double2(w.x.x - w.g3 * psn.x, w.x.y - w.g3 * psn.y);
-                        PS[o] = ps;
                         P[o] = make_double2(w.p.x + ps.x, w.p.y + ps.y);
-                        psn = ps;
-                    });
-    }
-    __syncthreads();
-
-    // ---------------- D2: v_corr (littleharsh.f90:896-993) ------------------
-    const double dtrk = dt * (rk.a + rk.b);
-    if (live && role < 2) {
-        double2 *U = role == 0 ? U1 : U3;
-        const double kd = dtrk * (role == 0 ? kxr : kzr);
-        double2 first = make_double2(0.0, 0.0), last = first, ps1 = first;
-        const RingW2 ring{warp_mem, lane};
-        stream_rows<RingW2::kDepth, 4>(nyu,
-                    [&](int r, int st) {
-                        const int j = r + 1;
-                        cp16(ring.at(st, 0), U + (size_t)j * nc);
-                        cp16(ring.at(st, 1), PS + (size_t)(j - 1) * nc);
-                    },
-                    [&](int r, int st) { return RowE{*ring.at(st, 0), *ring.at(st, 1), 0.0}; },
-                    [&](int r, const RowE &w) {
-                        const int j = r + 1;
-                        double2 a = w.a;
-                        const double2 ps = w.ps;
-                        a = make_double2(a.x - -(kd * ps.y), a.y - kd * ps.x);
-                        U[(size_t)j * nc] = a;
+                        const double2 a1 = make_double2(w.u1.x - -(kd1 * ps.y), w.u1.y - kd1 * ps.x);
+                        const double2 a3 = make_double2(w.u3.x - -(kd3 * ps.y), w.u3.y - kd3 * ps.x);
+                        U1[oj] = a1;
+                        U3[oj] = a3;
+                        if (j <= nyv) {
+                            const double mv = dtrk_u2 * w.th;
+                            U2[oj] = make_double2(w.u2.x - mv * (psn.x - ps.x), w.u2.y - mv * (psn.y - ps.y));
+                        }
+                        if (j == nyu) {
+                            last1 = a1;
+                            last3 = a3;
+                        }
                         if (j == 1) {
-                            first = a;
+                            first1 = a1;
+                            first3 = a3;
                             ps1 = ps;
                         }
-                        if (j == nyu) last = a;
+                        psn = ps;
                     });
-        U[0] = cscale(I.gwbc, first);
-        U[(size_t)(nyu + 1) * nc] = cscale(I.gwbc, last);
-        if (!isfinite(first.x) || !isfinite(first.y) || !isfinite(ps1.x) || !isfinite(ps1.y))
+        U1[0] = cscale(I.gwbc, first1);
+        U1[(size_t)(nyu + 1) * nc] = cscale(I.gwbc, last1);
+        U3[0] = cscale(I.gwbc, first3);
+        U3[(size_t)(nyu + 1) * nc] = cscale(I.gwbc, last3);
+        U2[0] = make_double2(0.0, 0.0);
+        U2[(size_t)(nyv + 1) * nc] = make_double2(0.0, 0.0);
+        if (!isfinite(first1.x) || !isfinite(first1.y) || !isfinite(first3.x) || !isfinite(first3.y) ||
+            !isfinite(ps1.x) || !isfinite(ps1.y))
             atomicOr(I.err, ERR_NONFINITE);
-        if (role == 0 && mean && kRK == 3) {
+        if (mean && kRK == 3) {
             // flowrateIm (littleharsh.f90:473-492) via meanflow_ctP (:572-589)
             __threadfence_block();
             double Qu = 0.0;
@@ -506,28 +507,6 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
             I.sc[SC_QX] = Qu;
             I.sc[SC_ITER] = I.sc[SC_ITER] + 1.0;
         }
-    } else if (live && role == 2) {
-        const double dtrk_u2 = dtrk * ddv;
-        double2 psc = PS[0];  // psi(j) of the current row
-        const RingW2 ring{warp_mem, lane};
-        stream_rows<RingW2::kDepth, 4>(nyv,
-                    [&](int r, int st) {
-                        const int j = r + 1;
-                        cp16(ring.at(st, 0), U2 + (size_t)j * nc);
-                        cp16(ring.at(st, 1), PS + (size_t)j * nc);  // psi(j+1)
-                    },
-                    [&](int r, int st) { return RowE{*ring.at(st, 0), *ring.at(st, 1), sthv[r + 1]}; },
-                    [&](int r, const RowE &w) {
-                        const int j = r + 1;
-                        double2 v = w.a;
-                        const double2 psn = w.ps;
-                        const double mv = dtrk_u2 * w.th;
-                        v = make_double2(v.x - mv * (psn.x - psc.x), v.y - mv * (psn.y - psc.y));
-                        U2[(size_t)j * nc] = v;
-                        psc = psn;
-                    });
-        U2[0] = make_double2(0.0, 0.0);
-        U2[(size_t)(nyv + 1) * nc] = make_double2(0.0, 0.0);
     }
 }
 

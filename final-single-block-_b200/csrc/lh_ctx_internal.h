@@ -12,6 +12,7 @@ struct lh_ctx {
     lh::Plan plan;
     lh::Inst *d_inst = nullptr;
     cudaStream_t st = nullptr;
+    int device = 0;            // the CUDA device current at lh_ctx_create
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     bool have_state = false;

@@ -299,40 +299,64 @@ ClassTiles fast_tiles(const HostSetup &s, int cbz_max, int rb, int cbf_max)
     int nb = (s.nxh + cbz_max - 1) / cbz_max;
     c.cbz = (s.nxh + nb - 1) / nb;
     c.tz = fast_threads(s.Mz, c.cbz);
-    c.smz = (size_t)s.Mz * c.cbz * sizeof(double2);
+    c.smz = zinv_smem(s.Mz, c.cbz);
     rb = std::max(1, std::min(rb, s.Mz));
     // the x stage's vectors sit at an odd row stride (3 rb rounded up to odd)
-    while (rb > 1 && !fits(1, s.Mx, 3 * rb, (3 * rb) | 1)) rb--;
+    while (rb > 1 && !(xprod_threads(s.Mx, rb) <= fast_max_threads(1) && xprod_smem(s.Mx, rb) <= smax)) rb--;
     c.rbx = rb;
-    c.tx = fast_threads(s.Mx, 3 * rb);
-    c.smx = (size_t)s.Mx * ((3 * rb) | 1) * sizeof(double2);
+    c.tx = xprod_threads(s.Mx, rb);
+    c.smx = xprod_smem(s.Mx, rb);
     cbf_max = std::max(1, std::min(cbf_max, s.nxh));
     // z forward: one half of the six products (3 vectors per x mode) per CTA
-    while (cbf_max > 1 && !fits(2, s.Mz, 3 * cbf_max, (3 * cbf_max) | 1)) cbf_max--;
+    while (cbf_max > 1 && !(zfwd_threads(s.Mz, cbf_max) <= fast_max_threads(2) && zfwd_smem(s.Mz, cbf_max) <= smax))
+        cbf_max--;
     nb = (s.nxh + cbf_max - 1) / cbf_max;
     c.cbf = (s.nxh + nb - 1) / nb;
-    c.tf = fast_threads(s.Mz, 3 * c.cbf);
-    c.smf = (size_t)s.Mz * ((3 * c.cbf) | 1) * sizeof(double2);
+    c.tf = zfwd_threads(s.Mz, c.cbf);
+    c.smf = zfwd_smem(s.Mz, c.cbf);
     return c;
 }
 
-ClassTiles class_tiles(const HostSetup &s, bool force_generic)
+// Default tile bounds of a fast size: measured on B200 at 128^2 (16 threads
+// per vector): 16 x modes per z-inverse CTA, 4 z rows per x CTA, up to 4 x
+// modes per z-forward CTA; sizes with fewer threads per vector take
+// proportionally more.  The z-forward bound is 80/vz, one less at Mz = 96
+// and 192 (ny = 153 sweeps: one x mode fewer was faster there, slower at
+// Mz = 288 and 384, even at 48).
+void default_bounds(const HostSetup &s, int &cbz, int &rbx, int &cbf)
+{
+    const int vz = std::max(1, fast_vector_threads(s.Mz)), vx = std::max(1, fast_vector_threads(s.Mx));
+    cbz = 256 / vz;
+    rbx = std::max(1, 64 / vx);
+    cbf = std::max(1, 80 / vz - ((s.Mz == 96 || s.Mz == 192) ? 1 : 0));
+}
+
+// Tile bounds of a class: the autotuner's candidate, else the environment
+// override LH_TILES=cbz,rbx,cbf, else the tuned table, else the defaults.
+ClassTiles class_tiles(const HostSetup &s, bool force_generic, const TuneParams *force)
 {
     ClassTiles c{};
     c.fast = !force_generic && fast_size(s.Mz) && fast_size(s.Mx);
-    const char *ov = getenv("LH_TILES");
-    int a = 0, b = 0, d = 0;
-    if (c.fast && ov && sscanf(ov, "%d,%d,%d", &a, &b, &d) == 3 && a > 0 && b > 0 && d > 0) return fast_tiles(s, a, b, d);
     if (c.fast) {
-        // measured on B200 at 128^2 (16 threads per vector): 16 x modes per
-        // z-inverse CTA, 4 z rows per x CTA, up to 4 x modes per z-forward
-        // CTA; sizes with fewer threads per vector take proportionally more.
-        // The z-forward bound is 80/vz, one less at Mz = 96 and 192 (ny =
-        // 153 sweeps: one x mode fewer was faster there, slower at Mz = 288
-        // and 384, even at 48).
-        const int vz = std::max(1, fast_vector_threads(s.Mz)), vx = std::max(1, fast_vector_threads(s.Mx));
-        const int cbf = std::max(1, 80 / vz - ((s.Mz == 96 || s.Mz == 192) ? 1 : 0));
-        c = fast_tiles(s, 256 / vz, std::max(1, 64 / vx), cbf);
+        int a = 0, b = 0, d = 0;
+        default_bounds(s, a, b, d);
+        TuneParams tp;
+        const char *ov = getenv("LH_TILES");
+        int oa = 0, ob = 0, od = 0;
+        if (force && force->cbz > 0) {
+            a = force->cbz;
+            b = force->rbx;
+            d = force->cbf;
+        } else if (ov && sscanf(ov, "%d,%d,%d", &oa, &ob, &od) == 3 && oa > 0 && ob > 0 && od > 0) {
+            a = oa;
+            b = ob;
+            d = od;
+        } else if (tune_lookup(s.Mz, s.Mx, s.nyu, tp) && tp.cbz > 0) {
+            a = tp.cbz;
+            b = tp.rbx;
+            d = tp.cbf;
+        }
+        c = fast_tiles(s, a, b, d);
     } else {
         Tiles t = default_tiles(s.Mx, s.Mz, s.nxh, s.nyu);
         c.cbz = t.bc_zinv;
@@ -347,7 +371,17 @@ ClassTiles class_tiles(const HostSetup &s, bool force_generic)
 }
 }  // namespace
 
-cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, bool force_generic)
+TuneParams default_params(const HostSetup &s)
+{
+    TuneParams t;
+    if (fast_size(s.Mz) && fast_size(s.Mx)) default_bounds(s, t.cbz, t.rbx, t.cbf);
+    t.staging_mb = (int)(staging_budget() >> 20);
+    t.col_waves = 1;
+    return t;
+}
+
+cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, bool force_generic,
+                       const TuneParams *force)
 {
     // the work buffer, side stream and events survive a rebuild
     p.rounds.clear();
@@ -375,8 +409,14 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
     std::vector<const HostSetup *> rep(ncls, nullptr);
     for (size_t q = 0; q < insts.size(); q++)
         if (!rep[cls_of[q]]) rep[cls_of[q]] = &insts[q]->hs;
-    for (size_t c = 0; c < ncls; c++) tiles[c] = class_tiles(*rep[c], force_generic);
-    const size_t l2_budget = staging_budget();
+    for (size_t c = 0; c < ncls; c++) tiles[c] = class_tiles(*rep[c], force_generic, force);
+    // staging budget and column-pass launches: the candidate, else the
+    // environment, else the tuned entry of a single-class plan, else defaults
+    TuneParams tuned;
+    const bool have_tuned = ncls == 1 && tune_lookup(rep[0]->Mz, rep[0]->Mx, rep[0]->nyu, tuned);
+    size_t l2_budget = staging_budget();
+    if (force && force->staging_mb > 0) l2_budget = (size_t)force->staging_mb << 20;
+    else if (!getenv("LH_STAGING_MB") && have_tuned && tuned.staging_mb > 0) l2_budget = (size_t)tuned.staging_mb << 20;
     std::vector<int> chunk_eff(insts.size());
     for (size_t q = 0; q < insts.size(); q++) {
         const HostSetup &s = insts[q]->hs;
@@ -403,6 +443,12 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
     const char *sc = getenv("LH_SMALL_COLUMNS");
     const long small_max = sc ? atol(sc) : kSmallColumnsDefault;
     p.col_small = (long)total_cols <= small_max;
+    // Column blocks split over this many back-to-back launches (LH_COLUMN_WAVES):
+    // fewer columns in flight keep the pass's intermediates in L2.
+    const char *cw = getenv("LH_COLUMN_WAVES");
+    p.col_waves = force && force->col_waves > 0 ? force->col_waves
+                  : cw ? std::max(1, atoi(cw))
+                  : (have_tuned && tuned.col_waves > 0 ? tuned.col_waves : 1);
     // work lists [round][stage][class]
     std::vector<std::vector<std::vector<std::vector<Work>>>> lists(
         rounds, std::vector<std::vector<std::vector<Work>>>(3, std::vector<std::vector<Work>>(ncls)));
@@ -601,8 +647,12 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
     if (p.col_small)
         k_column_small<<<(unsigned)p.column.size(), 32 * kSmallWarps, p.sm_col, st>>>(d_insts, p.d_work + p.off_column,
                                                                                       kRK);
-    else
-        k_column<<<(unsigned)p.column.size(), kColumnBlock, p.sm_col, st>>>(d_insts, p.d_work + p.off_column, kRK);
+    else {
+        const size_t nb = p.column.size(), per = (nb + p.col_waves - 1) / p.col_waves;
+        for (size_t b0 = 0; b0 < nb; b0 += per)
+            k_column<<<(unsigned)std::min(per, nb - b0), kColumnBlock, p.sm_col, st>>>(
+                d_insts, p.d_work + p.off_column + b0, kRK);
+    }
     if ((e = time_end(timer, 4, st)) != cudaSuccess) return e;
     return cudaGetLastError();
 }

@@ -96,6 +96,7 @@ struct Plan {
     size_t off_column = 0;
     size_t sm_col = 0;
     bool col_small = false;  // column pass by k_column_small (one CTA per column)
+    int col_waves = 1;       // column-pass launches the column blocks are split over
     int ninst = 0;
     bool force_generic = false;
     cudaStream_t side[kRoundStreams - 1] = {};  // rounds r % kRoundStreams != 0
@@ -110,7 +111,26 @@ struct LaunchTimer {
     int n[5] = {0, 0, 0, 0, 0};
 };
 
-cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, bool force_generic = false);
+// Launch-shape parameters of a size class that the autotuner (lh_tune.cu)
+// chooses: x modes per z-inverse CTA, z rows per x-products CTA, x modes per
+// z-forward CTA (upper bounds, clamped to each kernel's launch bounds and
+// shared memory), the plane-staging budget in MB and the number of
+// column-pass launches.  0 = the built-in default (or its environment
+// override).  None of them changes any arithmetic.
+struct TuneParams {
+    int cbz = 0, rbx = 0, cbf = 0, staging_mb = 0, col_waves = 0;
+};
+// The built-in defaults of a size, as numbers.
+TuneParams default_params(const HostSetup &s);
+// Process-wide table of tuned parameters keyed by (Mz, Mx, nyu); plan_build
+// consults it for every size class it has no environment override for.
+bool tune_lookup(int Mz, int Mx, int nyu, TuneParams &out);
+void tune_store(int Mz, int Mx, int nyu, const TuneParams &t);
+
+// `force` (the autotuner's candidate) takes precedence over the table and
+// the environment.
+cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, bool force_generic = false,
+                       const TuneParams *force = nullptr);
 void plan_free(Plan &p);
 // Enqueue one substep of every instance of the plan.
 cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl_any, cudaStream_t st,

@@ -45,6 +45,11 @@ bool fast_size(int n);
 int fast_threads(int n, int vectors);
 int fast_max_threads(int stage);  // launch-bounds block size of a fast stage
 int fast_vector_threads(int n);   // threads per vector of a fast length
+size_t zinv_smem(int n, int cb);  // shared memory of a z-inverse CTA of cb vectors
+int xprod_threads(int n, int rb);  // threads of an x-stage CTA of rb z rows
+size_t xprod_smem(int n, int rb);  // shared memory of an x-stage CTA of rb z rows
+int zfwd_threads(int n, int cb);   // threads of a z-forward CTA of cb x modes
+size_t zfwd_smem(int n, int cb);   // shared memory of a z-forward CTA of cb x modes
 cudaError_t fast_set_attributes(int Mz, int Mx, size_t smz, size_t smx, size_t smf);
 void fast_launch_zinv(int Mz, unsigned grid, int threads, size_t smem, cudaStream_t st, const Inst *insts,
                       const Work *work, int count, int cb);

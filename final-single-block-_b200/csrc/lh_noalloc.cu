@@ -66,10 +66,25 @@ extern "C" int lh_lusolu_noalloc(lh_ctx *c, int grid, int kRK, double dt, const 
                  " columns exceed the fixed scratch of " + std::to_string(kScratchDoubles) + " entries";
         return LH_EINVAL;
     }
+    // the scratch address is per device: the context's device must be current
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess && dev != c->device) {
+        c->err = "lh_lusolu_noalloc: device " + std::to_string(dev) + " is current, the context was created on device " +
+                 std::to_string(c->device);
+        return LH_EINVAL;
+    }
     double *scratch = nullptr;
-    cudaError_t e = scratch_on_current_device(&scratch);
+    if (e == cudaSuccess) e = scratch_on_current_device(&scratch);
     if (e != cudaSuccess) {
         c->err = std::string("lh_lusolu_noalloc: scratch lookup: ") + cudaGetErrorString(e);
+        return LH_ECUDA;
+    }
+    // an error left by earlier work on this thread is reported as such, not
+    // as this launch's
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        c->err = std::string("lh_lusolu_noalloc: earlier error on this thread: ") + cudaGetErrorString(e);
         return LH_ECUDA;
     }
     lh::k_lusolu<<<(s.nc + 127) / 128, 128, 0, c->st>>>(c->d_inst, grid, kRK, dt,

@@ -16,6 +16,8 @@
 // 373-418) are linear and commute with the z transform, so they are applied
 // to the z-transformed rows in the x stage: the z inverse runs on three
 // fields per plane instead of six.
+#include <cstdlib>
+
 #include "lh_fft.cuh"
 
 // Launch bounds (max threads, min resident CTAs per SM) each kernel's
@@ -122,6 +124,68 @@ __global__ void __launch_bounds__(LH_ZINV_T, LH_ZINV_B) k_zinv_f(const Inst *__r
                 for (int k2 = 0; k2 < N2; k2++) dst[(size_t)(r + N1 * k2) * nxh] = b[k2];
             }
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The same z inverse with the threads of a vector in one warp (vector-major:
+// thread t works on x mode t / VT, VT = max(N1, N2) in {8, 16}), so the
+// exchange between the two passes is warp-local: a __syncwarp instead of
+// block barriers, and the warps of a CTA never wait on one another.  The
+// N1 x N2 exchange matrix of a vector is stored with a padded row (N2 + 1)
+// so the column-wise reads of the second pass are free of bank conflicts.
+// Same arithmetic as k_zinv_f, element for element.
+template <int NZ>
+__global__ void __launch_bounds__(LH_ZINV_T, LH_ZINV_B) k_zinv_w(const Inst *__restrict__ insts, const Work *__restrict__ work,
+                                                         int count, int cb)
+{
+    constexpr int N1 = Plan2<NZ>::N1, N2 = Plan2<NZ>::N2;
+    constexpr int VT = N1 > N2 ? N1 : N2;
+    // sizes whose vectors do not fit a warp are never launched (zinv_warp_size)
+    if constexpr (32 % VT != 0) return;
+    constexpr int LD = N2 + 1;
+    constexpr int Nz = 2 * NZ / 3;
+    extern __shared__ double2 sm[];
+    if ((int)blockIdx.x >= count) return;
+    const double2 *tw = insts[work[blockIdx.x].inst].twz;
+    const int t = threadIdx.x, v = t / VT, r = t % VT;
+    const double2 twr = __ldg(tw + (r < N2 ? r : 0));
+    const Work w = work[blockIdx.x];
+    const Inst &I = insts[w.inst];
+    const int nxh = I.nxh, nc = I.nc;
+    const int nblk = (nxh + cb - 1) / cb;
+    const int f = w.blk / nblk, i = (w.blk % nblk) * cb + v;
+    const bool ok = v < cb && i < nxh;
+    double2 *T = sm + (size_t)(v < cb ? v : 0) * N1 * LD;
+    const double2 *src = (f == 0 ? I.U1 : (f == 1 ? I.U3 : I.U2)) + (size_t)w.j * nc;
+    if (v < cb && r < N2) {
+        double2 a[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; n1++) {
+            const int n = r + N2 * n1;
+            int kr = -1;
+            if (n < Nz / 2) kr = n;
+            else if (n >= NZ - Nz / 2) kr = n - (NZ - Nz);
+            a[n1] = (kr >= 0 && ok) ? src[kr * nxh + i] : make_double2(0.0, 0.0);
+        }
+        DFT<N1, +1, NZ>::run(a, tw);
+        TwStep ts(twr);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) {
+            double2 z = a[k1];
+            if (k1 > 0) z = twiddle<+1>(ts.next(), z);
+            T[k1 * LD + r] = z;
+        }
+    }
+    __syncwarp();
+    if (ok && r < N1) {
+        double2 b[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; n2++) b[n2] = T[r * LD + n2];
+        DFT<N2, +1, NZ>::run(b, tw);
+        double2 *dst = sin_field(I, w.slot, f) + i;
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) dst[(size_t)(r + N1 * k2) * nxh] = b[k2];
     }
 }
 
@@ -326,6 +390,203 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
 }
 
 // ---------------------------------------------------------------------------
+// The same x stage with the threads of a vector in one warp.  Vector v of a
+// CTA is (z row v / 3, pair v % 3); its VT = max(N1, N2) threads are
+// consecutive, so the gather, both transforms and the split of a vector
+// are warp-local (__syncwarp), and only the products, which combine the
+// three pairs of a row, synchronise -- the 96 threads of a row group (2
+// rows at VT = 16, 4 at VT = 8) on a named barrier of their own, so the
+// groups of a CTA never wait on one another.  Each vector owns one region
+// of max(NX, N1 (N2 + 1)) complex: natural order for the gather, the
+// products and the first pass's reads, an N1 x (N2 + 1) padded matrix for
+// the exchange between the passes (conflict-free column reads).  The CFL
+// maxima are reduced per warp.  Same arithmetic as k_xprod_f, element for
+// element.
+template <int NX>
+__global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_w(const Inst *__restrict__ insts, const Work *__restrict__ work,
+                                                          int count, int rb, int want_max)
+{
+    constexpr int N1 = Plan2<NX>::N1, N2 = Plan2<NX>::N2;
+    constexpr int VT = N1 > N2 ? N1 : N2;
+    if constexpr (32 % VT != 0) return;  // never launched (xprod_warp_size)
+    constexpr int LD = N2 + 1;
+    constexpr int REG = (NX > N1 * LD ? NX : N1 * LD);
+    constexpr int RG = 32 / VT;  // rows per 96-thread group
+    constexpr int nxh = NX / 3 + 1;
+    extern __shared__ double2 sm[];
+    if ((int)blockIdx.x >= count) return;
+    const double2 *tw = insts[work[blockIdx.x].inst].twx;
+    const int t = threadIdx.x, v = t / VT, r = t % VT;
+    const int row = v / 3, pair = v % 3, grp = row / RG;
+    const double2 twr = __ldg(tw + (r < N2 ? r : 0));
+    const Work w = work[blockIdx.x];
+    const Inst &I = insts[w.inst];
+    const int Mz = I.Mz, j = w.j;
+    const int q = w.blk * rb + row;  // this vector's z row
+    const bool live = row < rb;      // threads past the CTA's rows only join the barriers
+    const bool rowok = live && q < Mz;
+    double2 *z = sm + (size_t)(live ? v : 0) * REG;
+    const size_t fs = (size_t)Mz * nxh;
+    // (0) gather this vector's two real rows with the y interpolations
+    // (interp_v FOU3D.f90:407, interp_u :387) straight into the packed
+    // Hermitian-extended complex vector z = A + iB, natural order
+    if (live) {
+        const double2 *u1j = sin_field(I, w.aux + 1, 0), *u3j = u1j + fs, *vj = u3j + fs;
+        const double2 *vjm = sin_field(I, w.aux, 2);
+        const double2 *u1p = sin_field(I, w.aux + 2, 0), *u3p = u1p + fs;
+        const double dnv = 1.0 / (I.yv[j] - I.yv[j - 1]), dnu = 1.0 / (I.yu[j + 1] - I.yu[j]);
+        const double w0v = (I.yu[j] - I.yv[j - 1]) * dnv, w1v = (I.yv[j] - I.yu[j]) * dnv;
+        const double w0u = (I.yv[j] - I.yu[j]) * dnu, w1u = (I.yu[j + 1] - I.yv[j]) * dnu;
+        for (int k = r; k < nxh; k += VT) {
+            double2 A = make_double2(0.0, 0.0), B = A;
+            if (rowok) {
+                const size_t o = (size_t)q * nxh + k;
+                if (pair == 0) {
+                    A = u1j[o];
+                    B = u3j[o];
+                } else if (pair == 1) {
+                    const double2 x0 = vj[o], x1 = vjm[o];
+                    A = make_double2(w0v * x0.x + w1v * x1.x, w0v * x0.y + w1v * x1.y);
+                    B = x0;
+                } else {
+                    const double2 a0 = u1p[o], a1 = u1j[o], b0 = u3p[o], b1 = u3j[o];
+                    A = make_double2(w0u * a0.x + w1u * a1.x, w0u * a0.y + w1u * a1.y);
+                    B = make_double2(w0u * b0.x + w1u * b1.x, w0u * b0.y + w1u * b1.y);
+                }
+            }
+            if (k == 0) {
+                z[0] = make_double2(A.x, B.x);
+            } else {
+                z[k] = make_double2(A.x - B.y, A.y + B.x);
+                z[NX - k] = make_double2(A.x + B.y, B.x - A.y);
+            }
+        }
+        for (int x = nxh + r; x <= NX - nxh; x += VT) z[x] = make_double2(0.0, 0.0);
+    }
+    __syncwarp();
+    // (1) inverse pass 1: lane r < N2 holds n = r + N2 n1; out to the padded matrix
+    {
+        double2 a[N1];
+        if (live && r < N2) {
+#pragma unroll
+            for (int n1 = 0; n1 < N1; n1++) a[n1] = z[r + N2 * n1];
+        }
+        __syncwarp();
+        if (live && r < N2) {
+            DFT<N1, +1, NX>::run(a, tw);
+            TwStep ts(twr);
+#pragma unroll
+            for (int k1 = 0; k1 < N1; k1++) {
+                double2 y = a[k1];
+                if (k1 > 0) y = twiddle<+1>(ts.next(), y);
+                z[k1 * LD + r] = y;
+            }
+        }
+    }
+    __syncwarp();
+    // (2) inverse pass 2 -> physical values z[x], natural order
+    {
+        double2 b[N2];
+        if (live && r < N1) {
+#pragma unroll
+            for (int n2 = 0; n2 < N2; n2++) b[n2] = z[r * LD + n2];
+            DFT<N2, +1, NX>::run(b, tw);
+        }
+        __syncwarp();
+        if (live && r < N1) {
+#pragma unroll
+            for (int k2 = 0; k2 < N2; k2++) z[r + N1 * k2] = b[k2];
+        }
+    }
+    // (3) products of each row group's rows (the three pairs of a row sit in
+    // up to two warps of the group); CFL maxima over planes 1..nyu-1
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(96) : "memory");
+    const bool track = want_max && I.dt_mode == 0 && j <= I.nyu - 1;
+    double m1 = 0.0, m3 = 0.0;
+    {
+        const int gt = t - grp * 96;  // thread within the group
+        const int row0 = grp * RG;
+        for (int e = gt; e < RG * NX; e += 96) {
+            const int rr = row0 + e / NX, x = e % NX;
+            if (rr >= rb) continue;
+            double2 *p0 = sm + (size_t)(3 * rr) * REG + x, *p1 = p0 + REG, *p2 = p1 + REG;
+            const double2 a0 = *p0, a1 = *p1, a2 = *p2;
+            const double u1 = a0.x, u3 = a0.y, u2c = a1.x, u2 = a1.y, u1f = a2.x, u3f = a2.y;
+            if (track && w.blk * rb + rr < Mz) {
+                m1 = fmax(m1, fabs(u1));
+                m3 = fmax(m3, fabs(u3));
+            }
+            *p0 = make_double2(u1 * u1, u1 * u3);
+            *p1 = make_double2(u2c * u2c, u3 * u3);
+            *p2 = make_double2(u1f * u2, u3f * u2);
+        }
+    }
+    if (track) {
+        for (int o = 16; o > 0; o >>= 1) {
+            m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+            m3 = fmax(m3, __shfl_xor_sync(0xffffffffu, m3, o));
+        }
+        if ((t & 31) == 0) {
+            atomicMax(reinterpret_cast<unsigned long long *>(&I.sc[SC_U1MAX]), (unsigned long long)__double_as_longlong(m1));
+            atomicMax(reinterpret_cast<unsigned long long *>(&I.sc[SC_U3MAX]), (unsigned long long)__double_as_longlong(m3));
+        }
+    }
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(96) : "memory");
+    // (4) forward pass 1
+    {
+        double2 a[N1];
+        if (live && r < N2) {
+#pragma unroll
+            for (int n1 = 0; n1 < N1; n1++) a[n1] = z[r + N2 * n1];
+            DFT<N1, -1, NX>::run(a, tw);
+        }
+        __syncwarp();
+        if (live && r < N2) {
+            TwStep ts(twr);
+#pragma unroll
+            for (int k1 = 0; k1 < N1; k1++) {
+                double2 y = a[k1];
+                if (k1 > 0) y = twiddle<-1>(ts.next(), y);
+                z[k1 * LD + r] = y;
+            }
+        }
+    }
+    __syncwarp();
+    // (5) forward pass 2 -> X[k], natural order
+    {
+        double2 b[N2];
+        if (live && r < N1) {
+#pragma unroll
+            for (int n2 = 0; n2 < N2; n2++) b[n2] = z[r * LD + n2];
+            DFT<N2, -1, NX>::run(b, tw);
+        }
+        __syncwarp();
+        if (live && r < N1) {
+#pragma unroll
+            for (int k2 = 0; k2 < N2; k2++) z[r + N1 * k2] = b[k2];
+        }
+    }
+    __syncwarp();
+    // (6) split the packed real transforms, scale 1/Mx, keep modes i <= Nx/2
+    if (rowok) {
+        double2 *S = sprod_slot(I, w.slot);
+        const double dn1 = 1.0 / NX;
+        for (int k = r; k < nxh; k += VT) {
+            const double2 zk = z[k];
+            const double2 zm = z[k == 0 ? 0 : NX - k];
+            double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+            double2 B = make_double2(0.5 * (zk.y + zm.y), 0.5 * (zm.x - zk.x));
+            if (k == 0) {
+                A.y = 0.0;
+                B.y = 0.0;
+            }
+            S[((size_t)(2 * pair) * Mz + q) * nxh + k] = make_double2(dn1 * A.x, dn1 * A.y);
+            S[((size_t)(2 * pair + 1) * Mz + q) * nxh + k] = make_double2(dn1 * B.x, dn1 * B.y);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // z forward, masks and derivatives of one (plane, block of cb x modes, half):
 // phys_to_four_du's cft (FOU3D.f90:1654-1672), der_x/der_z (:420-523) and
 // planes_to_modes_UVP/NUVP.  The six products split into two independent
@@ -416,6 +677,103 @@ __global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_f(const Inst *__r
 }
 
 // ---------------------------------------------------------------------------
+// The same z forward with the threads of a vector in one warp.  Vector v is
+// (product f = v / cb, x mode c = v % cb), so the two vectors of a warp are
+// neighbouring x modes of one product and its loads of a z row share their
+// sectors.  Both transform passes are warp-local (__syncwarp); one block
+// barrier precedes the masks and derivatives, which combine the three
+// products of an x mode.  Each vector owns one region of max(NZ, N1 (N2+1))
+// complex (the padded exchange matrix, then the scaled spectrum in natural
+// order).  Same arithmetic as k_zfwd_f, element for element.
+template <int NZ>
+__global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_w(const Inst *__restrict__ insts, const Work *__restrict__ work,
+                                                         int count, int cb)
+{
+    constexpr int N1 = Plan2<NZ>::N1, N2 = Plan2<NZ>::N2;
+    constexpr int VT = N1 > N2 ? N1 : N2;
+    if constexpr (32 % VT != 0) return;  // never launched (zfwd_warp_size)
+    constexpr int LD = N2 + 1;
+    constexpr int REG = (NZ > N1 * LD ? NZ : N1 * LD);
+    constexpr int Nz = 2 * NZ / 3;
+    extern __shared__ double2 sm[];
+    if ((int)blockIdx.x >= count) return;
+    const double2 *tw = insts[work[blockIdx.x].inst].twz;
+    const int t = threadIdx.x, v = t / VT, r = t % VT;
+    const int f = v / cb, c = v % cb;
+    const bool live = f < 3;
+    const double2 twr = __ldg(tw + (r < N2 ? r : 0));
+    const Work w = work[blockIdx.x];
+    const Inst &I = insts[w.inst];
+    const int nxh = I.nxh, nc = I.nc, j = w.j;
+    const int h = w.blk & 1;
+    const int i0 = (w.blk >> 1) * cb, i = i0 + c;
+    const int g = h == 0 ? (f == 2 ? 3 : f) : (f == 0 ? 2 : f + 3);  // product of this vector
+    const double2 *S = sprod_slot(I, w.slot);
+    const bool ok = live && i < nxh;
+    double2 *z = sm + (size_t)(live ? v : 0) * REG;
+    {
+        double2 a[N1];
+        if (live && r < N2) {
+#pragma unroll
+            for (int n1 = 0; n1 < N1; n1++)
+                a[n1] = ok ? S[((size_t)g * NZ + r + N2 * n1) * nxh + i] : make_double2(0.0, 0.0);
+            DFT<N1, -1, NZ>::run(a, tw);
+            TwStep ts(twr);
+#pragma unroll
+            for (int k1 = 0; k1 < N1; k1++) {
+                double2 y = a[k1];
+                if (k1 > 0) y = twiddle<-1>(ts.next(), y);
+                z[k1 * LD + r] = y;
+            }
+        }
+    }
+    __syncwarp();
+    {
+        double2 b[N2];
+        if (live && r < N1) {
+#pragma unroll
+            for (int n2 = 0; n2 < N2; n2++) b[n2] = z[r * LD + n2];
+            DFT<N2, -1, NZ>::run(b, tw);
+        }
+        __syncwarp();
+        if (live && r < N1) {
+            const double dn1 = 1.0 / NZ;
+#pragma unroll
+            for (int k2 = 0; k2 < N2; k2++) z[r + N1 * k2] = make_double2(dn1 * b[k2].x, dn1 * b[k2].y);
+        }
+    }
+    __syncthreads();
+    const FastDiv by_cb(cb);
+    for (int e = t; e < Nz * cb; e += blockDim.x) {
+        const int kr = by_cb.div(e), cc = by_cb.mod(e, kr), ii = i0 + cc;
+        if (ii >= nxh) continue;
+        const int zp = kr < Nz / 2 ? kr : kr + NZ - Nz;
+        const double2 p0 = sm[(size_t)cc * REG + zp], p1 = sm[(size_t)(cb + cc) * REG + zp],
+                      p2 = sm[(size_t)(2 * cb + cc) * REG + zp];
+        const size_t on = (size_t)(j - 1) * nc + kr * nxh + ii;
+        const bool keep = kr != Nz / 2;  // der_x/der_z zero the kz = -Nz/2 row (FOU3D.f90:444-447)
+        const double kx = I.kx[ii], kz = I.kz[kr];
+        if (h == 0) {  // p0 uu, p1 uw, p2 ww
+            double2 n1 = make_double2(0.0, 0.0), n3 = n1;
+            if (keep) {
+                n1 = make_double2(-(kx * p0.y) + -(kz * p1.y), kx * p0.x + kz * p1.x);
+                n3 = make_double2(-(kx * p1.y) + -(kz * p2.y), kx * p1.x + kz * p2.x);
+            }
+            I.NXZ1[on] = n1;
+            I.NXZ3[on] = n3;
+        } else {  // p0 vv, p1 uv, p2 wv
+            const size_t o = (size_t)j * nc + kr * nxh + ii;
+            I.VVC[o] = p0;
+            I.UVF[o] = p1;
+            I.WVF[o] = p2;
+            double2 n2 = make_double2(0.0, 0.0);
+            if (keep) n2 = make_double2(-(kx * p1.y) + -(kz * p2.y), kx * p1.x + kz * p2.x);
+            I.NXZ2[on] = n2;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host dispatch
 int fast_max_threads(int stage) { return stage == 0 ? LH_ZINV_T : (stage == 1 ? LH_XPROD_T : LH_ZFWD_T); }
 
@@ -463,6 +821,106 @@ int fast_threads(int n, int vectors)
     return ((t + 31) / 32) * 32;
 }
 
+// z-inverse sizes whose vectors fit a warp (max(N1, N2) divides 32), and
+// whether the warp-local variant is selected (LH_ZINV_WARP=1).
+bool zinv_warp_size(int n)
+{
+    switch (n) {
+#define LH_CASE(N) \
+    case N:        \
+        return 32 % (Plan2<N>::N1 > Plan2<N>::N2 ? Plan2<N>::N1 : Plan2<N>::N2) == 0;
+        LH_FAST_SIZES(LH_CASE)
+#undef LH_CASE
+    default:
+        return false;
+    }
+}
+
+bool zinv_warp(int n)
+{
+    const char *ev = getenv("LH_ZINV_WARP");
+    return ev && ev[0] == '1' && zinv_warp_size(n);
+}
+
+// x stage: sizes whose vectors fit a warp, and the LH_XPROD_WARP=1 selection
+bool xprod_warp_size(int n) { return zinv_warp_size(n); }
+bool xprod_warp(int n)
+{
+    const char *ev = getenv("LH_XPROD_WARP");
+    return ev && ev[0] == '1' && xprod_warp_size(n);
+}
+
+// Threads and shared memory of an x-stage CTA of rb z rows: the warp variant
+// runs 96-thread row groups (32 / VT rows each), one region per vector.
+int xprod_threads(int n, int rb)
+{
+    if (!xprod_warp(n)) return fast_threads(n, 3 * rb);
+    const int vt = fast_vector_threads(n), rg = 32 / vt;
+    return 96 * ((rb + rg - 1) / rg);
+}
+
+size_t xprod_smem(int n, int rb)
+{
+    if (!xprod_warp(n)) return (size_t)n * ((3 * rb) | 1) * sizeof(double2);
+    switch (n) {
+#define LH_CASE(N)                                                                                  \
+    case N: {                                                                                       \
+        const int reg = N > Plan2<N>::N1 * (Plan2<N>::N2 + 1) ? N : Plan2<N>::N1 * (Plan2<N>::N2 + 1); \
+        const int rg = 32 / fast_vector_threads(N);                                                 \
+        return (size_t)3 * rg * ((rb + rg - 1) / rg) * reg * sizeof(double2);                     \
+    }
+        LH_FAST_SIZES(LH_CASE)
+#undef LH_CASE
+    default:
+        return 0;
+    }
+}
+
+// z forward: sizes whose vectors fit a warp, the LH_ZFWD_WARP=1 selection,
+// threads and shared memory of a CTA of cb x modes (3 cb vectors)
+bool zfwd_warp(int n)
+{
+    const char *ev = getenv("LH_ZFWD_WARP");
+    return ev && ev[0] == '1' && zinv_warp_size(n);
+}
+
+int zfwd_threads(int n, int cb)
+{
+    if (!zfwd_warp(n)) return fast_threads(n, 3 * cb);
+    return ((3 * cb * fast_vector_threads(n) + 31) / 32) * 32;
+}
+
+size_t zfwd_smem(int n, int cb)
+{
+    if (!zfwd_warp(n)) return (size_t)n * ((3 * cb) | 1) * sizeof(double2);
+    switch (n) {
+#define LH_CASE(N)                                                                                  \
+    case N: {                                                                                       \
+        const int reg = N > Plan2<N>::N1 * (Plan2<N>::N2 + 1) ? N : Plan2<N>::N1 * (Plan2<N>::N2 + 1); \
+        return (size_t)3 * cb * reg * sizeof(double2);                                            \
+    }
+        LH_FAST_SIZES(LH_CASE)
+#undef LH_CASE
+    default:
+        return 0;
+    }
+}
+
+// Shared memory of a z-inverse CTA of cb vectors.
+size_t zinv_smem(int n, int cb)
+{
+    if (!zinv_warp(n)) return (size_t)n * cb * sizeof(double2);
+    switch (n) {
+#define LH_CASE(N) \
+    case N:        \
+        return (size_t)cb * Plan2<N>::N1 * (Plan2<N>::N2 + 1) * sizeof(double2);
+        LH_FAST_SIZES(LH_CASE)
+#undef LH_CASE
+    default:
+        return 0;
+    }
+}
+
 cudaError_t fast_set_attributes(int Mz, int Mx, size_t smz, size_t smx, size_t smf)
 {
     cudaError_t e = cudaSuccess;
@@ -470,7 +928,9 @@ cudaError_t fast_set_attributes(int Mz, int Mx, size_t smz, size_t smx, size_t s
 #define LH_CASE(N)                                        \
     case N:                                               \
         e = raise_smem_limit((const void *)k_zinv_f<N>, smz); \
+        if (e == cudaSuccess) e = raise_smem_limit((const void *)k_zinv_w<N>, smz); \
         if (e == cudaSuccess) e = raise_smem_limit((const void *)k_zfwd_f<N>, smf); \
+        if (e == cudaSuccess) e = raise_smem_limit((const void *)k_zfwd_w<N>, smf); \
         break;
         LH_FAST_SIZES(LH_CASE)
 #undef LH_CASE
@@ -482,6 +942,7 @@ cudaError_t fast_set_attributes(int Mz, int Mx, size_t smz, size_t smx, size_t s
 #define LH_CASE(N)                                         \
     case N:                                                \
         e = raise_smem_limit((const void *)k_xprod_f<N>, smx); \
+        if (e == cudaSuccess) e = raise_smem_limit((const void *)k_xprod_w<N>, smx); \
         break;
         LH_FAST_SIZES(LH_CASE)
 #undef LH_CASE
@@ -497,7 +958,8 @@ void fast_launch_zinv(int Mz, unsigned grid, int threads, size_t smem, cudaStrea
     switch (Mz) {
 #define LH_CASE(N)                                                                   \
     case N:                                                                          \
-        k_zinv_f<N><<<grid, threads, smem, st>>>(insts, work, count, cb);            \
+        if (zinv_warp(N)) k_zinv_w<N><<<grid, threads, smem, st>>>(insts, work, count, cb); \
+        else k_zinv_f<N><<<grid, threads, smem, st>>>(insts, work, count, cb);       \
         break;
         LH_FAST_SIZES(LH_CASE)
 #undef LH_CASE
@@ -510,7 +972,8 @@ void fast_launch_xprod(int Mx, unsigned grid, int threads, size_t smem, cudaStre
     switch (Mx) {
 #define LH_CASE(N)                                                                   \
     case N:                                                                          \
-        k_xprod_f<N><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); \
+        if (xprod_warp(N)) k_xprod_w<N><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); \
+        else k_xprod_f<N><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); \
         break;
         LH_FAST_SIZES(LH_CASE)
 #undef LH_CASE
@@ -523,7 +986,8 @@ void fast_launch_zfwd(int Mz, unsigned grid, int threads, size_t smem, cudaStrea
     switch (Mz) {
 #define LH_CASE(N)                                                                   \
     case N:                                                                          \
-        k_zfwd_f<N><<<grid, threads, smem, st>>>(insts, work, count, cb);            \
+        if (zfwd_warp(N)) k_zfwd_w<N><<<grid, threads, smem, st>>>(insts, work, count, cb); \
+        else k_zfwd_f<N><<<grid, threads, smem, st>>>(insts, work, count, cb);       \
         break;
         LH_FAST_SIZES(LH_CASE)
 #undef LH_CASE

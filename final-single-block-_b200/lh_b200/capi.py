@@ -31,6 +31,7 @@ EXPORTS = [
     "lh_batch_download", "lh_batch_scalars", "lh_batch_count", "lh_batch_synchronize",
     "lh_spectra_accumulate", "lh_spectra_reset", "lh_get_spectra",
     "lh_stats_accumulate", "lh_stats_reset", "lh_get_stats", "lh_pressure_snapshot", "lh_omega_x",
+    "lh_tridiag_factor", "lh_tridiag_solve", "lh_set_dg", "lh_set_scalars", "lh_autotune",
 ]
 
 
@@ -151,6 +152,11 @@ def lib() -> ctypes.CDLL:
         "lh_get_stats": (i, [v, dp, sz, P(i)]),
         "lh_pressure_snapshot": (i, [v]),
         "lh_omega_x": (i, [v, dp, sz]),
+        "lh_tridiag_factor": (i, [v, i, i, d, dp, sz]),
+        "lh_tridiag_solve": (i, [v, i, dp, dp]),
+        "lh_set_dg": (i, [v, dp]),
+        "lh_set_scalars": (i, [v, d, i, d]),
+        "lh_autotune": (i, [v, i, P(i)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -357,6 +363,40 @@ class Engine:
         a = col_layout(x).copy()
         self._ck(self.L.lh_lusolp(self.h, _dp(a)), "lusolp")
         return a
+
+    def tridiag_factor(self, grid: int, kRK: int = 1, dt: float = 0.0) -> np.ndarray:
+        """Factors a(3, j, column) as an array [column, j, 3] (LU_build +
+        LU_dec, or DG for grid 3)."""
+        n = self.L.lh_tridiag_factor(self.h, grid, kRK, dt, None, 0)
+        if n < 0:
+            self._ck(n, "tridiag_factor")
+        a = np.zeros(n)
+        rc = self.L.lh_tridiag_factor(self.h, grid, kRK, dt, _dp(a), n)
+        if rc < 0:
+            self._ck(rc, "tridiag_factor")
+        return a.reshape(self.sizes.ncols, -1, 3)
+
+    def tridiag_solve(self, grid: int, a: np.ndarray, x: np.ndarray) -> np.ndarray:
+        fa = np.ascontiguousarray(a, np.float64)
+        xb = col_layout(x).copy()
+        self._ck(self.L.lh_tridiag_solve(self.h, grid, _dp(fa), _dp(xb)), "tridiag_solve")
+        return xb
+
+    def set_dg(self, a: np.ndarray):
+        self._ck(self.L.lh_set_dg(self.h, _dp(np.ascontiguousarray(a, np.float64))), "set_dg")
+
+    def set_scalars(self, t: float, it: int, mpgx: float):
+        """Continue a run: t, iter and mpgx of a restart file (getini, flag_init = 2)."""
+        self._ck(self.L.lh_set_scalars(self.h, float(t), int(it), float(mpgx)), "set_scalars")
+
+    def autotune(self, force: bool = False) -> dict:
+        """Tune this size's launch shapes (or read them from the cache)."""
+        out = (ctypes.c_int * 6)()
+        self._ck(self.L.lh_autotune(self.h, 1 if force else 0, out), "autotune")
+        keys = ("cbz", "rbx", "cbf", "staging_mb", "col_waves")
+        r = {k: out[i] for i, k in enumerate(keys)}
+        r["source"] = {1: "measured", 2: "cache"}.get(out[5], "?")
+        return r
 
     def grid(self, which: int) -> np.ndarray:
         n = self.L.lh_get_grid(self.h, which, None, 0)

@@ -11,13 +11,20 @@ exactly the steps the batch takes while it is a member), so no device
 round trip decides completion.  Results are the final states and the
 time-to-completion of every request.
 
+Host work stays off the device's critical path: initial states of arrived
+requests are built by a worker thread while the device steps the live
+instances, and the batch uploads an admission on a stream of its own while
+queued steps run (it synchronises only to rebuild its step graph).
+
 ``run_plain`` runs the same requests one at a time through the
-single-instance :class:`Engine` -- the drop-in path -- for comparison.
+single-instance :class:`Engine` -- the drop-in path -- on the same arrival
+clock, for comparison.
 """
 from __future__ import annotations
 
 import math
 import time
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -84,67 +91,95 @@ class ServeStats:
 
 def serve(requests, hbm_budget: int, max_chunk: int = 50, keep_results: bool = True,
           time_scale: float = 1.0, clock=time.perf_counter, batch_factory=Batch,
-          state_fn=None) -> ServeStats:
+          state_fn=None, prefetch: int = 4) -> ServeStats:
     """Continuous batching over `requests` (sorted by arrival).
 
     time_scale < 1 compresses the arrival times (a faster replay of the
-    stream); the reported time-to-completion is in real seconds.
+    stream); the reported time-to-completion is in real seconds.  Up to
+    `prefetch` arrived requests have their initial states built ahead by a
+    worker thread (0: built on the scheduling thread at admission).
     batch_factory/state_fn default to the device batch and the synthetic
     initial state; tests substitute host fakes to check the scheduling.
     """
     reqs = sorted(requests, key=lambda r: r.arrival)
     state_fn = state_fn or initial_state
     b = batch_factory(hbm_budget)
+    pool = ThreadPoolExecutor(max_workers=1) if prefetch > 0 else None
+    pending: dict[int, object] = {}  # rid -> future of the initial state
     queue: list[Request] = []
     live: dict[int, tuple[Request, int]] = {}  # slot -> (request, remaining steps)
     nxt = 0
     t0 = clock()
     live_samples = []
     done = 0
-    while done < len(reqs):
-        now = clock() - t0
-        while nxt < len(reqs) and reqs[nxt].arrival * time_scale <= now:
-            queue.append(reqs[nxt])
-            nxt += 1
-        # admit in arrival order while memory allows
-        while queue:
-            r = queue[0]
-            try:
-                slot = b.add(r.desc, *state_fn(r))
-            except LHError as e:
-                if e.code == LH_ENOMEM and live:
-                    break  # wait for a retirement
-                raise
-            r.admitted = clock() - t0
-            live[slot] = (r, r.nsteps)
-            queue.pop(0)
-        if not live:
-            # idle until the next arrival
-            if nxt < len(reqs):
-                wait = reqs[nxt].arrival * time_scale - (clock() - t0)
-                if wait > 0:
-                    time.sleep(min(wait, 0.05))
-            continue
-        k = min(max_chunk, min(rem for _, rem in live.values()))
-        b.step(k)
-        live_samples.append(len(live))
-        finished = []
-        for slot, (r, rem) in list(live.items()):
-            rem -= k
-            if rem == 0:
-                finished.append(slot)
-            live[slot] = (r, rem)
-        if finished:
-            b.synchronize()
-            tf = clock() - t0
-            for slot in finished:
-                r, _ = live.pop(slot)
-                if keep_results:
-                    r.result = b.download(slot)
-                r.finished = tf
-                b.remove(slot)
-                done += 1
-    b.synchronize()
+
+    def state_of(r: Request, block: bool):
+        if pool is None:
+            return state_fn(r)
+        f = pending.get(r.rid)
+        if f is None:
+            f = pending[r.rid] = pool.submit(state_fn, r)
+        if not block and not f.done():
+            return None
+        return f.result()
+
+    try:
+        while done < len(reqs):
+            now = clock() - t0
+            while nxt < len(reqs) and reqs[nxt].arrival * time_scale <= now:
+                queue.append(reqs[nxt])
+                nxt += 1
+            if pool is not None:
+                for r in queue[:prefetch]:
+                    if r.rid not in pending:
+                        pending[r.rid] = pool.submit(state_fn, r)
+            # admit in arrival order while memory allows; with instances live,
+            # a state still being built waits for the next round
+            while queue:
+                r = queue[0]
+                st = state_of(r, block=not live)
+                if st is None:
+                    break
+                try:
+                    slot = b.add(r.desc, *st)
+                except LHError as e:
+                    if e.code == LH_ENOMEM and live:
+                        break  # wait for a retirement
+                    raise
+                pending.pop(r.rid, None)
+                r.admitted = clock() - t0
+                live[slot] = (r, r.nsteps)
+                queue.pop(0)
+            if not live:
+                # idle until the next arrival
+                if nxt < len(reqs):
+                    wait = reqs[nxt].arrival * time_scale - (clock() - t0)
+                    if wait > 0:
+                        time.sleep(min(wait, 0.05))
+                continue
+            k = min(max_chunk, min(rem for _, rem in live.values()))
+            b.step(k)
+            live_samples.append(len(live))
+            finished = []
+            for slot, (r, rem) in list(live.items()):
+                rem -= k
+                if rem == 0:
+                    finished.append(slot)
+                live[slot] = (r, rem)
+            if finished:
+                b.synchronize()
+                tf = clock() - t0
+                for slot in finished:
+                    r, _ = live.pop(slot)
+                    if keep_results:
+                        r.result = b.download(slot)
+                    r.finished = tf
+                    b.remove(slot)
+                    done += 1
+        b.synchronize()
+    finally:
+        if pool is not None:
+            pool.shutdown(wait=True, cancel_futures=True)
     wall = clock() - t0
     ttc = [r.finished - r.arrival * time_scale for r in reqs]
     b.close()
@@ -154,17 +189,24 @@ def serve(requests, hbm_budget: int, max_chunk: int = 50, keep_results: bool = T
                       max_live=max(live_samples) if live_samples else 0, ttc=ttc)
 
 
-def run_plain(requests, keep_results: bool = True, clock=time.perf_counter) -> float:
-    """The drop-in path: each request alone through the single-instance engine.
+def run_plain(requests, keep_results: bool = True, clock=time.perf_counter, time_scale: float = 1.0) -> float:
+    """The drop-in path: each request alone through the single-instance engine,
+    in arrival order, none started before its arrival (the same clock as
+    :func:`serve`, so the two wall times compare like for like).
 
-    Returns the wall time; states go to ``request.result``."""
+    Returns the wall time; states go to ``request.result``, completion times
+    to ``request.finished``."""
     t0 = clock()
-    for r in requests:
+    for r in sorted(requests, key=lambda q: q.arrival):
+        wait = r.arrival * time_scale - (clock() - t0)
+        if wait > 0:
+            time.sleep(wait)
         e = Engine(r.desc)
         e.upload(*initial_state(r))
         e.step(r.nsteps)
         e.synchronize()
         if keep_results:
             r.result = e.download()
+        r.finished = clock() - t0
         e.close()
     return clock() - t0

@@ -57,7 +57,7 @@ def _reqs():
 def test_every_request_runs_exactly_its_steps():
     FakeBatch.instances.clear()
     reqs = _reqs()
-    st = serve(reqs, hbm_budget=0, max_chunk=4, batch_factory=FakeBatch, state_fn=lambda r: ())
+    st = serve(reqs, hbm_budget=0, max_chunk=4, batch_factory=FakeBatch, state_fn=lambda r: (), prefetch=0)
     assert st.requests == 5
     for r in reqs:
         assert r.result["steps"] == r.nsteps
@@ -71,7 +71,7 @@ def test_budget_defers_admission_until_memory_frees():
     FakeBatch.instances.clear()
     reqs = _reqs()
     budget = Desc(Nx=16, Nz=16, ny=33).points() + Desc(Nx=8, Nz=8, ny=17).points()
-    st = serve(reqs, hbm_budget=budget, max_chunk=50, batch_factory=FakeBatch, state_fn=lambda r: ())
+    st = serve(reqs, hbm_budget=budget, max_chunk=50, batch_factory=FakeBatch, state_fn=lambda r: (), prefetch=0)
     for r in reqs:
         assert r.result["steps"] == r.nsteps
     log = FakeBatch.instances[-1].log
@@ -89,7 +89,7 @@ def test_late_arrivals_join_while_others_run():
         return t["now"]
 
     reqs = [Request(0, d, 1, 40, 0.0), Request(1, d, 2, 5, 0.05)]
-    serve(reqs, hbm_budget=0, max_chunk=2, batch_factory=FakeBatch, state_fn=lambda r: (), clock=clock)
+    serve(reqs, hbm_budget=0, max_chunk=2, batch_factory=FakeBatch, state_fn=lambda r: (), clock=clock, prefetch=0)
     log = FakeBatch.instances[-1].log
     adds = [i for i, e in enumerate(log) if e[0] == "add"]
     steps = [i for i, e in enumerate(log) if e[0] == "step"]
@@ -103,4 +103,23 @@ def test_non_budget_errors_propagate():
         def add(self, desc, *state):
             raise LHError(-1, "bad size")
     with pytest.raises(LHError):
-        serve(_reqs(), hbm_budget=0, batch_factory=Broken, state_fn=lambda r: ())
+        serve(_reqs(), hbm_budget=0, batch_factory=Broken, state_fn=lambda r: (), prefetch=0)
+
+
+def test_prefetched_states_run_exactly_their_steps():
+    """With initial states built ahead by the worker thread the admissions may
+    fall into later rounds, but every request still runs exactly its steps,
+    with the state its own request produced."""
+    FakeBatch.instances.clear()
+    reqs = _reqs()
+    seen = []
+
+    def state_fn(r):
+        seen.append(r.rid)
+        return (r.rid,)
+
+    st = serve(reqs, hbm_budget=0, max_chunk=3, batch_factory=FakeBatch, state_fn=state_fn, prefetch=2)
+    assert st.requests == 5 and sorted(seen) == [0, 1, 2, 3, 4]
+    for r in reqs:
+        assert r.result["steps"] == r.nsteps
+        assert r.finished >= r.admitted
