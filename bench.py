@@ -243,6 +243,31 @@ def _batch_rate(b, pts, K):
     return pts * 3 * K / bt, 1e3 * bt / K
 
 
+def plain_small():
+    """The first configuration: one 32x32x153 instance, dt = 1e-3, Re_tau = 180,
+    device-resident, CUDA events on the engine's stream (it fits in L2)."""
+    import torch
+    from lh_b200 import Desc, Engine, grids, perturbed_laminar, re_from_retau
+    d = Desc(Nx=32, Nz=32, ny=153, Re=re_from_retau(RE_TAU, MPGX), mpgx=MPGX, dt_mode=1, dt=1e-3)
+    e = Engine(d)
+    e.upload(*perturbed_laminar(d, 20260001, *grids(d)))
+    e.step(5)
+    e.synchronize()
+    st = torch.cuda.ExternalStream(e.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    K = 100
+    a.record(st)
+    e.step(K)
+    b.record(st)
+    b.synchronize()
+    e.synchronize()
+    ms = a.elapsed_time(b) / K
+    e.close()
+    return {"workload": "plain, one 32x32x153 instance, dt 1e-3, Re_tau 180, 100 timed steps (the configuration's "
+                        "100-step run), state L2-resident", "value": d.points() * 3 / (ms * 1e-3), "unit": UNIT,
+            "ms_per_step": ms}
+
+
 def batched_and_served(args):
     """Throughput of the batched engine on the uniform batch (64 instances of
     32x32x153, Re_tau and dt drawn per instance) and on the uneven batch (16 x
@@ -403,8 +428,9 @@ def run_ours(args, rank, world, local_rank):
     (e2e_ms,) = max_over_ranks([ev2.elapsed_time(ev3)], world, "cuda")
     e2e_val = job_rate(world, pts_sub * Ke, e2e_ms * 1e-3)
 
-    batched = uneven = served = None
+    batched = uneven = served = small = None
     if rank == 0 and world == 1 and not args.no_serve:
+        small = plain_small()
         batched, uneven, served = batched_and_served(args)
 
     fp64 = None
@@ -439,6 +465,7 @@ def run_ours(args, rank, world, local_rank):
             "kernels": kernels,
             "dominant_kernel": dom[0],
             "cpu_baseline": cpu,
+            "plain_32x32x153": small,
             "batched": batched,
             "batched_uneven": uneven,
             "served": served,
@@ -461,7 +488,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=30)
     ap.add_argument("--serve-full-steps", action="store_true",
                     help="served stream with the configuration's step counts log-U[200,5000] (default 20..200)")
-    ap.add_argument("--serve-time-scale", type=float, default=0.25,
+    ap.add_argument("--serve-time-scale", type=float, default=0.05,
                     help="arrival times are replayed at this factor (<1: compressed)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -325,6 +325,20 @@ extern "C" int lh_batch_scalars(lh_batch *b, int slot, double *t, double *dt, in
     return LH_OK;
 }
 
+extern "C" int lh_batch_set_scalars(lh_batch *b, int slot, double t, int iter, double mpgx)
+{
+    if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot] || iter < 0)
+        return bfail(b, LH_EINVAL, "bad arguments");
+    const Inst &I = b->slots[slot]->inst;
+    const double v[3] = {t, mpgx, (double)iter};
+    // queued steps may still advance this instance: ordered after them
+    BCK(cudaMemcpyAsync(I.sc + SC_T, &v[0], sizeof(double), cudaMemcpyHostToDevice, b->st), "set scalars");
+    BCK(cudaMemcpyAsync(I.sc + SC_MPGX, &v[1], sizeof(double), cudaMemcpyHostToDevice, b->st), "set scalars");
+    BCK(cudaMemcpyAsync(I.sc + SC_ITER, &v[2], sizeof(double), cudaMemcpyHostToDevice, b->st), "set scalars");
+    BCK(cudaStreamSynchronize(b->st), "set scalars");
+    return LH_OK;
+}
+
 extern "C" int lh_batch_count(const lh_batch *b)
 {
     if (!b) return 0;

@@ -28,7 +28,7 @@ EXPORTS = [
     "lh_error_div", "lh_get_intermediate", "lh_four_to_phys", "lh_phys_to_four", "lh_lusolu",
     "lh_lusolp", "lh_lusolu_noalloc", "lh_batch_create", "lh_batch_destroy", "lh_batch_last_error",
     "lh_instance_bytes", "lh_batch_add", "lh_batch_remove", "lh_batch_step",
-    "lh_batch_download", "lh_batch_scalars", "lh_batch_count", "lh_batch_synchronize",
+    "lh_batch_download", "lh_batch_scalars", "lh_batch_set_scalars", "lh_batch_count", "lh_batch_synchronize",
     "lh_spectra_accumulate", "lh_spectra_reset", "lh_get_spectra",
     "lh_stats_accumulate", "lh_stats_reset", "lh_get_stats", "lh_pressure_snapshot", "lh_omega_x",
     "lh_tridiag_factor", "lh_tridiag_solve", "lh_set_dg", "lh_set_scalars", "lh_autotune",
@@ -142,6 +142,7 @@ def lib() -> ctypes.CDLL:
         "lh_batch_step": (i, [v, i]),
         "lh_batch_download": (i, [v, i, dp, dp, dp, dp]),
         "lh_batch_scalars": (i, [v, i, dp, dp, P(i)]),
+        "lh_batch_set_scalars": (i, [v, i, d, i, d]),
         "lh_batch_count": (i, [v]),
         "lh_batch_synchronize": (i, [v]),
         "lh_spectra_accumulate": (i, [v]),
@@ -457,6 +458,10 @@ class Batch:
 
     def count(self) -> int:
         return self.L.lh_batch_count(self.h)
+
+    def set_scalars(self, slot: int, t: float, it: int, mpgx: float):
+        """Restore t, iter and mpgx of an instance (a snapshot or restart file)."""
+        self._ck(self.L.lh_batch_set_scalars(self.h, slot, float(t), int(it), float(mpgx)), "set_scalars")
 
     def download(self, slot: int):
         d = self.desc[slot]

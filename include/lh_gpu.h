@@ -267,6 +267,11 @@ int lh_batch_step(lh_batch *b, int nsteps);
 int lh_batch_download(lh_batch *b, int slot, double *u1, double *u2,
                       double *u3, double *p);
 int lh_batch_scalars(lh_batch *b, int slot, double *t, double *dt, int *iter);
+/* Restore a snapshot of a live instance (lh_batch_download + lh_batch_scalars,
+ * or a restart file): set t, iter and mpgx of an admitted instance, as
+ * lh_set_scalars does for a context (getini with flag_init = 2,
+ * start.f90:1268-1282). */
+int lh_batch_set_scalars(lh_batch *b, int slot, double t, int iter, double mpgx);
 int lh_batch_count(const lh_batch *b);
 int lh_batch_synchronize(lh_batch *b);
 

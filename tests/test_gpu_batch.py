@@ -132,3 +132,61 @@ def test_batch_of_small_instances_uses_the_per_column_pass(monkeypatch):
         got = b.download(s)
         for f in ("u1", "u2", "u3", "p"):
             assert rel_l2(got[f], ref[f]) <= 1e-14, (d, f, rel_l2(got[f], ref[f]))
+
+
+def test_batch_snapshot_restore_continues_bit_for_bit():
+    """A live instance's snapshot (download + scalars) re-admitted into another
+    batch with its t and iter restored continues exactly as the instance does
+    where it was left (ct. pressure gradient: Nu of the previous substep
+    enters with c_1 = 0 at kRK = 1, so a step boundary carries no other state)."""
+    import numpy as np
+    from lh_b200 import Batch, Desc
+    d1 = Desc(Nx=32, Nz=32, ny=97, dt_mode=1, dt=1e-3)
+    d2 = Desc(Nx=64, Nz=32, ny=65, dt_mode=0, CFL=0.5)
+    a = Batch()
+    s1 = a.add(d1, *_ic(d1, 21))
+    a.add(d2, *_ic(d2, 22))
+    a.step(3)
+    a.synchronize()
+    snap, sc = a.download(s1), a.scalars(s1)
+    a.step(3)
+    a.synchronize()
+    want, want_sc = a.download(s1), a.scalars(s1)
+    b = Batch()
+    s = b.add(d1, snap["u1"], snap["u2"], snap["u3"], snap["p"])
+    b.set_scalars(s, sc["t"], sc["iter"], d1.mpgx)
+    b.step(3)
+    b.synchronize()
+    got, got_sc = b.download(s), b.scalars(s)
+    for f in ("u1", "u2", "u3", "p"):
+        assert np.array_equal(got[f], want[f]), f
+    assert got_sc == want_sc
+    a.close()
+    b.close()
+
+
+def test_uneven_batch_with_a_256x257_instance_equals_alone():
+    """The largest instance of the uneven configuration (256x256x257, tanh(2)
+    grid) in a batch with small ones gets a launch plan of its own and steps
+    exactly as it does alone (its single-instance step is checked against the
+    oracle in test_gpu_parity.py)."""
+    import numpy as np
+    from lh_b200 import Batch, Desc, Engine, re_from_retau
+    big = Desc(Nx=256, Nz=256, ny=257, grid_type=1, Re=re_from_retau(550), dt_mode=1, dt=2.5e-4)
+    small = Desc(Nx=32, Nz=32, ny=153, grid_type=1, Re=re_from_retau(180), dt_mode=1, dt=5e-4)
+    ics = [_ic(big, 31), _ic(small, 32), _ic(small, 33)]
+    b = Batch()
+    slots = [b.add(d, *ic) for d, ic in zip((big, small, small), ics)]
+    b.step(1)
+    b.synchronize()
+    for d, s, ic in zip((big, small, small), slots, ics):
+        e = Engine(d)
+        e.upload(*ic)
+        e.step(1)
+        e.synchronize()
+        ref = e.download()
+        got = b.download(s)
+        for f in ("u1", "u2", "u3", "p"):
+            assert np.array_equal(got[f], ref[f]), (d.Nx, f)
+        e.close()
+    b.close()
