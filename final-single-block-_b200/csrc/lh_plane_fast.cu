@@ -402,7 +402,12 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *
 // the exchange between the passes (conflict-free column reads).  The CFL
 // maxima are reduced per warp.  Same arithmetic as k_xprod_f, element for
 // element.
-template <int NX>
+//
+// DIRECT = 1: the first pass reads its N1 elements of the packed vector
+// straight from the staging rows in global memory (each mode's two rows are
+// read by the two lanes holding z[k] and z[NX - k]), so the gather's shared
+// memory round trip and its __syncwarp disappear.
+template <int NX, int DIRECT>
 __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_w(const Inst *__restrict__ insts, const Work *__restrict__ work,
                                                           int count, int rb, int want_max)
 {
@@ -427,33 +432,35 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_w(const Inst *
     const bool rowok = live && q < Mz;
     double2 *z = sm + (size_t)(live ? v : 0) * REG;
     const size_t fs = (size_t)Mz * nxh;
-    // (0) gather this vector's two real rows with the y interpolations
-    // (interp_v FOU3D.f90:407, interp_u :387) straight into the packed
-    // Hermitian-extended complex vector z = A + iB, natural order
-    if (live) {
-        const double2 *u1j = sin_field(I, w.aux + 1, 0), *u3j = u1j + fs, *vj = u3j + fs;
-        const double2 *vjm = sin_field(I, w.aux, 2);
-        const double2 *u1p = sin_field(I, w.aux + 2, 0), *u3p = u1p + fs;
-        const double dnv = 1.0 / (I.yv[j] - I.yv[j - 1]), dnu = 1.0 / (I.yu[j + 1] - I.yu[j]);
-        const double w0v = (I.yu[j] - I.yv[j - 1]) * dnv, w1v = (I.yv[j] - I.yu[j]) * dnv;
-        const double w0u = (I.yv[j] - I.yu[j]) * dnu, w1u = (I.yu[j + 1] - I.yv[j]) * dnu;
+    // (0) this vector's two real rows with the y interpolations (interp_v
+    // FOU3D.f90:407, interp_u :387) as the packed Hermitian-extended complex
+    // vector z = A + iB: z[0] = (A0.x, B0.x), z[k] = A_k + iB_k and
+    // z[NX - k] = conj(A_k) + i conj(B_k) for 0 < k <= Nx/2, zero between
+    const double2 *u1j = sin_field(I, w.aux + 1, 0), *u3j = u1j + fs, *vj = u3j + fs;
+    const double2 *vjm = sin_field(I, w.aux, 2);
+    const double2 *u1p = sin_field(I, w.aux + 2, 0), *u3p = u1p + fs;
+    const double dnv = 1.0 / (I.yv[j] - I.yv[j - 1]), dnu = 1.0 / (I.yu[j + 1] - I.yu[j]);
+    const double w0v = (I.yu[j] - I.yv[j - 1]) * dnv, w1v = (I.yv[j] - I.yu[j]) * dnv;
+    const double w0u = (I.yv[j] - I.yu[j]) * dnu, w1u = (I.yu[j + 1] - I.yv[j]) * dnu;
+    auto rows_at = [&](int k, double2 &A, double2 &B) {
+        const size_t o = (size_t)q * nxh + k;
+        if (pair == 0) {
+            A = u1j[o];
+            B = u3j[o];
+        } else if (pair == 1) {
+            const double2 x0 = vj[o], x1 = vjm[o];
+            A = make_double2(w0v * x0.x + w1v * x1.x, w0v * x0.y + w1v * x1.y);
+            B = x0;
+        } else {
+            const double2 a0 = u1p[o], a1 = u1j[o], b0 = u3p[o], b1 = u3j[o];
+            A = make_double2(w0u * a0.x + w1u * a1.x, w0u * a0.y + w1u * a1.y);
+            B = make_double2(w0u * b0.x + w1u * b1.x, w0u * b0.y + w1u * b1.y);
+        }
+    };
+    if (!DIRECT && live) {
         for (int k = r; k < nxh; k += VT) {
             double2 A = make_double2(0.0, 0.0), B = A;
-            if (rowok) {
-                const size_t o = (size_t)q * nxh + k;
-                if (pair == 0) {
-                    A = u1j[o];
-                    B = u3j[o];
-                } else if (pair == 1) {
-                    const double2 x0 = vj[o], x1 = vjm[o];
-                    A = make_double2(w0v * x0.x + w1v * x1.x, w0v * x0.y + w1v * x1.y);
-                    B = x0;
-                } else {
-                    const double2 a0 = u1p[o], a1 = u1j[o], b0 = u3p[o], b1 = u3j[o];
-                    A = make_double2(w0u * a0.x + w1u * a1.x, w0u * a0.y + w1u * a1.y);
-                    B = make_double2(w0u * b0.x + w1u * b1.x, w0u * b0.y + w1u * b1.y);
-                }
-            }
+            if (rowok) rows_at(k, A, B);
             if (k == 0) {
                 z[0] = make_double2(A.x, B.x);
             } else {
@@ -463,15 +470,31 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_w(const Inst *
         }
         for (int x = nxh + r; x <= NX - nxh; x += VT) z[x] = make_double2(0.0, 0.0);
     }
-    __syncwarp();
+    if (!DIRECT) __syncwarp();
     // (1) inverse pass 1: lane r < N2 holds n = r + N2 n1; out to the padded matrix
     {
         double2 a[N1];
         if (live && r < N2) {
+            if (DIRECT) {
 #pragma unroll
-            for (int n1 = 0; n1 < N1; n1++) a[n1] = z[r + N2 * n1];
+                for (int n1 = 0; n1 < N1; n1++) {
+                    const int n = r + N2 * n1;
+                    double2 A = make_double2(0.0, 0.0), B = A, y = A;
+                    if (rowok && n < nxh) {
+                        rows_at(n, A, B);
+                        y = n == 0 ? make_double2(A.x, B.x) : make_double2(A.x - B.y, A.y + B.x);
+                    } else if (rowok && n > NX - nxh) {
+                        rows_at(NX - n, A, B);
+                        y = make_double2(A.x + B.y, B.x - A.y);
+                    }
+                    a[n1] = y;
+                }
+            } else {
+#pragma unroll
+                for (int n1 = 0; n1 < N1; n1++) a[n1] = z[r + N2 * n1];
+            }
         }
-        __syncwarp();
+        if (!DIRECT) __syncwarp();
         if (live && r < N2) {
             DFT<N1, +1, NX>::run(a, tw);
             TwStep ts(twr);
@@ -847,7 +870,12 @@ bool xprod_warp_size(int n) { return zinv_warp_size(n); }
 bool xprod_warp(int n)
 {
     const char *ev = getenv("LH_XPROD_WARP");
-    return ev && ev[0] == '1' && xprod_warp_size(n);
+    return ev && (ev[0] == '1' || ev[0] == '2') && xprod_warp_size(n);
+}
+bool xprod_direct()
+{
+    const char *ev = getenv("LH_XPROD_WARP");
+    return ev && ev[0] == '2';
 }
 
 // Threads and shared memory of an x-stage CTA of rb z rows: the warp variant
@@ -942,7 +970,8 @@ cudaError_t fast_set_attributes(int Mz, int Mx, size_t smz, size_t smx, size_t s
 #define LH_CASE(N)                                         \
     case N:                                                \
         e = raise_smem_limit((const void *)k_xprod_f<N>, smx); \
-        if (e == cudaSuccess) e = raise_smem_limit((const void *)k_xprod_w<N>, smx); \
+        if (e == cudaSuccess) e = raise_smem_limit((const void *)k_xprod_w<N, 0>, smx); \
+        if (e == cudaSuccess) e = raise_smem_limit((const void *)k_xprod_w<N, 1>, smx); \
         break;
         LH_FAST_SIZES(LH_CASE)
 #undef LH_CASE
@@ -972,7 +1001,8 @@ void fast_launch_xprod(int Mx, unsigned grid, int threads, size_t smem, cudaStre
     switch (Mx) {
 #define LH_CASE(N)                                                                   \
     case N:                                                                          \
-        if (xprod_warp(N)) k_xprod_w<N><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); \
+        if (xprod_warp(N) && xprod_direct()) k_xprod_w<N, 1><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); \
+        else if (xprod_warp(N)) k_xprod_w<N, 0><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); \
         else k_xprod_f<N><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); \
         break;
         LH_FAST_SIZES(LH_CASE)
