@@ -96,15 +96,17 @@ def serve(requests, hbm_budget: int, max_chunk: int = 50, keep_results: bool = T
 
     time_scale < 1 compresses the arrival times (a faster replay of the
     stream); the reported time-to-completion is in real seconds.  Up to
-    `prefetch` arrived requests have their initial states built ahead by a
-    worker thread (0: built on the scheduling thread at admission).
+    `prefetch` arrived requests have their initial states built ahead by
+    worker threads while the device steps (0: built on the scheduling thread
+    at admission); admission itself is unchanged: every arrived request that
+    fits the budget joins before the next step.
     batch_factory/state_fn default to the device batch and the synthetic
     initial state; tests substitute host fakes to check the scheduling.
     """
     reqs = sorted(requests, key=lambda r: r.arrival)
     state_fn = state_fn or initial_state
     b = batch_factory(hbm_budget)
-    pool = ThreadPoolExecutor(max_workers=1) if prefetch > 0 else None
+    pool = ThreadPoolExecutor(max_workers=2) if prefetch > 0 else None
     pending: dict[int, object] = {}  # rid -> future of the initial state
     queue: list[Request] = []
     live: dict[int, tuple[Request, int]] = {}  # slot -> (request, remaining steps)
@@ -133,13 +135,13 @@ def serve(requests, hbm_budget: int, max_chunk: int = 50, keep_results: bool = T
                 for r in queue[:prefetch]:
                     if r.rid not in pending:
                         pending[r.rid] = pool.submit(state_fn, r)
-            # admit in arrival order while memory allows; with instances live,
-            # a state still being built waits for the next round
+            # admit every arrived request in arrival order while memory allows
+            # (a state the worker has started is waited for: it costs no more
+            # than building it here, and the worker builds the next ones while
+            # the device steps)
             while queue:
                 r = queue[0]
-                st = state_of(r, block=not live)
-                if st is None:
-                    break
+                st = state_of(r, block=True)
                 try:
                     slot = b.add(r.desc, *st)
                 except LHError as e:
