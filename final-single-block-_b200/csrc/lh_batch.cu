@@ -1,20 +1,23 @@
 // Batched engine: many independent channel instances of uneven size advance
 // together.  Every substep issues the same kernels as a single instance, but
-// each launch's work table spans all live instances (instance, plane, block),
-// so a batch of N instances costs one launch per kernel class and chunk
-// round rather than N.  Each instance owns its device allocation; admission
-// is checked against an HBM budget.  One RK3 step of the current membership
-// is captured once in a CUDA graph and replayed until membership changes.
+// each launch's work table spans all instances of a launch group (instance,
+// plane, block), so a group of N instances costs one launch per kernel
+// class and chunk round rather than N.  Each instance owns its device
+// allocation; admission is checked against an HBM budget.
 //
 // Instances of at least kIsolateModes Fourier modes (Nx*Nz) keep the GPU
 // busy on their own; sharing launches with others only shrinks their L2
-// staging share and splits their rounds, so each gets its own launch plan
-// (its chunk rounds sized as if alone), while the smaller instances share
-// one plan.  The plans' launches follow one another on the batch stream
-// inside the same captured step.
+// staging share and splits their rounds, so each forms a launch group of its
+// own (its chunk rounds sized as if alone), while the smaller instances
+// share one group.  Every group keeps its own plan, instance table and CUDA
+// graph of one RK3 step; a batch step replays the groups' graphs one after
+// another on the batch stream.  When membership changes, only the groups
+// whose members changed are planned and captured again -- an admission or a
+// retirement of a large instance leaves every other group's graph as it was.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstdlib>
 #include <memory>
 #include <new>
@@ -30,18 +33,22 @@ using namespace lh;
 struct lh_batch {
     size_t budget = 0, used = 0;
     std::vector<std::unique_ptr<DevInstance>> slots;  // nullptr = free slot
-    std::vector<int> live;                            // slot ids in launch order
-    std::vector<Plan> plans;                          // plan groups (see above)
-    std::vector<int> plan_off;                        // first instance of each group in d_insts
-    std::vector<bool> plan_cfl;                       // a CFL-mode instance in the group
-    Inst *d_insts = nullptr;
-    size_t d_insts_cap = 0;
+    std::vector<uint64_t> serial;                     // admission number of each slot's instance
+    uint64_t next_serial = 1;
+    // one launch group: its members (admission numbers, launch order), plan,
+    // device instance table and captured RK3 step
+    struct Group {
+        std::vector<uint64_t> key;
+        Plan plan;
+        Inst *d_inst = nullptr;
+        bool cfl = false;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t gexec = nullptr;
+    };
+    std::vector<std::unique_ptr<Group>> groups;
     cudaStream_t st = nullptr;
     cudaStream_t st_up = nullptr;  // admissions upload here while steps run on st
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
     bool dirty = true;
-    bool any_cfl = false;
     std::string err;
     // device blocks of retired instances, reused by later admissions so a
     // request stream does not pay cudaMalloc/cudaFree (a device-wide
@@ -84,12 +91,15 @@ static int bcuda(lh_batch *b, cudaError_t e, const char *where)
         if (e_ != cudaSuccess) return bcuda(b, e_, where);      \
     } while (0)
 
-static void drop_graph(lh_batch *b)
+static void free_group(lh_batch::Group &g)
 {
-    if (b->gexec) cudaGraphExecDestroy(b->gexec);
-    if (b->graph) cudaGraphDestroy(b->graph);
-    b->gexec = nullptr;
-    b->graph = nullptr;
+    if (g.gexec) cudaGraphExecDestroy(g.gexec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g.gexec = nullptr;
+    g.graph = nullptr;
+    plan_free(g.plan);
+    if (g.d_inst) cudaFree(g.d_inst);
+    g.d_inst = nullptr;
 }
 
 extern "C" int lh_batch_create(size_t budget, lh_batch **out)
@@ -118,9 +128,8 @@ extern "C" int lh_batch_destroy(lh_batch *b)
 {
     if (!b) return LH_OK;
     if (b->st) cudaStreamSynchronize(b->st);
-    drop_graph(b);
-    for (Plan &p : b->plans) plan_free(p);
-    if (b->d_insts) cudaFree(b->d_insts);
+    for (auto &g : b->groups) free_group(*g);
+    b->groups.clear();
     for (auto &s : b->slots)
         if (s) instance_free(*s);
     pool_release(b, 0);
@@ -196,6 +205,8 @@ extern "C" int lh_batch_add(lh_batch *b, const lh_grid_desc *desc, const double 
         b->slots.emplace_back();
     }
     b->slots[id] = std::move(d);
+    if (b->serial.size() < b->slots.size()) b->serial.resize(b->slots.size(), 0);
+    b->serial[id] = b->next_serial++;
     b->dirty = true;
     *slot = id;
     return LH_OK;
@@ -223,71 +234,62 @@ extern "C" int lh_batch_remove(lh_batch *b, int slot)
 static int rebuild(lh_batch *b)
 {
     if (!b->dirty) return LH_OK;
-    // queued steps still read the work tables and the instance table that
-    // are rewritten below
+    // queued steps still read the plans and instance tables of groups that
+    // are freed below
     BCK(cudaStreamSynchronize(b->st), "synchronize");
-    drop_graph(b);
-    b->live.clear();
-    b->any_cfl = false;
     const char *iso = getenv("LH_BATCH_ISOLATE");
     const long isolate = iso ? atol(iso) : kIsolateModes;
     // groups: the shared group of the smaller instances first, then one group
-    // per isolated instance; d_insts holds the instances in that order
-    std::vector<std::vector<int>> groups(1);
+    // per isolated instance
+    std::vector<std::vector<int>> members(1);
     for (size_t k = 0; k < b->slots.size(); k++)
         if (b->slots[k]) {
             const HostSetup &hs = b->slots[k]->hs;
-            if ((long)hs.Nx * hs.Nz >= isolate) groups.push_back({(int)k});
-            else groups[0].push_back((int)k);
+            if ((long)hs.Nx * hs.Nz >= isolate) members.push_back({(int)k});
+            else members[0].push_back((int)k);
         }
-    if (groups[0].empty()) groups.erase(groups.begin());
-    std::vector<Inst> hi;
-    b->plan_off.clear();
-    b->plan_cfl.clear();
-    for (const auto &g : groups) {
-        b->plan_off.push_back((int)hi.size());
-        bool cfl = false;
-        for (int k : g) {
-            b->live.push_back(k);
-            hi.push_back(b->slots[k]->inst);
-            cfl |= b->slots[k]->desc.dt_mode == LH_DT_CFL;
+    if (members[0].empty()) members.erase(members.begin());
+    std::vector<std::unique_ptr<lh_batch::Group>> next;
+    for (const auto &m : members) {
+        std::vector<uint64_t> key;
+        for (int k : m) key.push_back(b->serial[k]);
+        // a group with the same instances keeps its plan and graph
+        auto it = std::find_if(b->groups.begin(), b->groups.end(),
+                               [&](const std::unique_ptr<lh_batch::Group> &g) { return g && g->key == key; });
+        if (it != b->groups.end()) {
+            next.push_back(std::move(*it));
+            continue;
         }
-        b->plan_cfl.push_back(cfl);
-        b->any_cfl |= cfl;
-    }
-    if (hi.empty()) {
-        b->dirty = false;
-        return LH_OK;
-    }
-    if (hi.size() > b->d_insts_cap) {
-        if (b->d_insts) cudaFree(b->d_insts);
-        b->d_insts = nullptr;
-        BCK(cudaMalloc(&b->d_insts, hi.size() * sizeof(Inst)), "alloc instance table");
-        b->d_insts_cap = hi.size();
-    }
-    BCK(cudaMemcpy(b->d_insts, hi.data(), hi.size() * sizeof(Inst), cudaMemcpyHostToDevice), "instance table");
-    // plans (their work buffers, streams and events) are kept and rebuilt in place
-    while (b->plans.size() > groups.size()) {
-        plan_free(b->plans.back());
-        b->plans.pop_back();
-    }
-    b->plans.resize(groups.size());
-    for (size_t g = 0; g < groups.size(); g++) {
+        auto g = std::unique_ptr<lh_batch::Group>(new (std::nothrow) lh_batch::Group());
+        if (!g) return bfail(b, LH_ENOMEM, "host allocation");
+        g->key = key;
+        std::vector<Inst> hi;
         std::vector<const DevInstance *> v;
-        for (int k : groups[g]) v.push_back(b->slots[k].get());
-        BCK(plan_build(b->plans[g], v), "plan");
+        for (int k : m) {
+            hi.push_back(b->slots[k]->inst);
+            v.push_back(b->slots[k].get());
+            g->cfl |= b->slots[k]->desc.dt_mode == LH_DT_CFL;
+        }
+        cudaError_t e = cudaMalloc(&g->d_inst, hi.size() * sizeof(Inst));
+        if (e == cudaSuccess) e = cudaMemcpy(g->d_inst, hi.data(), hi.size() * sizeof(Inst), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = plan_build(g->plan, v);
+        if (e == cudaSuccess) e = cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaError_t el = cudaSuccess;
+            for (int kk = 1; kk <= 3 && el == cudaSuccess; kk++) el = launch_substep(g->plan, g->d_inst, kk, g->cfl, b->st);
+            cudaError_t ee = cudaStreamEndCapture(b->st, &g->graph);
+            e = el != cudaSuccess ? el : ee;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&g->gexec, g->graph, 0);
+        if (e != cudaSuccess) {
+            free_group(*g);
+            return bcuda(b, e, "group plan");
+        }
+        next.push_back(std::move(g));
     }
-    BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal), "capture");
-    cudaError_t el = cudaSuccess;
-    for (int k = 1; k <= 3 && el == cudaSuccess; k++)
-        for (size_t g = 0; g < b->plans.size() && el == cudaSuccess; g++)
-            el = launch_substep(b->plans[g], b->d_insts + b->plan_off[g], k, b->plan_cfl[g], b->st);
-    cudaGraph_t gr = nullptr;
-    cudaError_t ee = cudaStreamEndCapture(b->st, &gr);
-    if (el != cudaSuccess) return bcuda(b, el, "capture launch");
-    if (ee != cudaSuccess) return bcuda(b, ee, "capture end");
-    b->graph = gr;
-    BCK(cudaGraphInstantiate(&b->gexec, gr, 0), "instantiate");
+    for (auto &g : b->groups)
+        if (g) free_group(*g);
+    b->groups = std::move(next);
     b->dirty = false;
     return LH_OK;
 }
@@ -297,8 +299,8 @@ extern "C" int lh_batch_step(lh_batch *b, int nsteps)
     if (!b || nsteps < 0) return bfail(b, LH_EINVAL, "bad arguments");
     int rc = rebuild(b);
     if (rc) return rc;
-    if (b->live.empty()) return LH_OK;
-    for (int s = 0; s < nsteps; s++) BCK(cudaGraphLaunch(b->gexec, b->st), "graph launch");
+    for (int s = 0; s < nsteps; s++)
+        for (auto &g : b->groups) BCK(cudaGraphLaunch(g->gexec, b->st), "graph launch");
     return LH_OK;
 }
 
