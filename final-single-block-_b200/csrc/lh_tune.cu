@@ -118,7 +118,7 @@ void cache_append(const std::string &key, const TuneParams &t, double ms)
 }
 
 // ms per RK3 step of a plan on the scratch instance: one warm step, then
-// enough steps for at least ~2 ms of device time.
+// enough steps for at least ~8 ms of device time.
 cudaError_t time_plan(const Plan &p, const Inst *d_inst, bool cfl, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1,
                       double &ms)
 {
@@ -135,7 +135,7 @@ cudaError_t time_plan(const Plan &p, const Inst *d_inst, bool cfl, cudaStream_t 
         if ((e = cudaEventSynchronize(e1)) != cudaSuccess) return e;
         float f = 0.f;
         cudaEventElapsedTime(&f, e0, e1);
-        if (f >= 2.0f || reps >= 64) {
+        if (f >= 8.0f || reps >= 256) {
             ms = f / reps;
             return cudaSuccess;
         }
