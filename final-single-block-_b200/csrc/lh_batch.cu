@@ -10,8 +10,9 @@
 // staging share and splits their rounds, so each forms a launch group of its
 // own (its chunk rounds sized as if alone), while the smaller instances
 // share one group.  Every group keeps its own plan, instance table and CUDA
-// graph of one RK3 step; a batch step replays the groups' graphs one after
-// another on the batch stream.  When membership changes, only the groups
+// graph of one RK3 step; a batch step replays the groups' graphs on up to
+// four streams at once (forked from the batch stream and joined back), so a
+// large instance's latency-bound kernels overlap the others'.  When membership changes, only the groups
 // whose members changed are planned and captured again -- an admission or a
 // retirement of a large instance leaves every other group's graph as it was.
 #include <cuda_runtime.h>
@@ -48,6 +49,11 @@ struct lh_batch {
     std::vector<std::unique_ptr<Group>> groups;
     cudaStream_t st = nullptr;
     cudaStream_t st_up = nullptr;  // admissions upload here while steps run on st
+    // the launch groups run concurrently on these streams, forked from st and
+    // joined back at every step (they touch disjoint instances)
+    static constexpr int kGroupStreams = 4;
+    cudaStream_t gst[kGroupStreams] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kGroupStreams] = {};
     bool dirty = true;
     std::string err;
     // device blocks of retired instances, reused by later admissions so a
@@ -115,9 +121,13 @@ extern "C" int lh_batch_create(size_t budget, lh_batch **out)
         delete b;
         return LH_ECUDA;
     }
-    if (cudaStreamCreateWithFlags(&b->st_up, cudaStreamNonBlocking) != cudaSuccess) {
-        cudaStreamDestroy(b->st);
-        delete b;
+    bool ok = cudaStreamCreateWithFlags(&b->st_up, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; k < lh_batch::kGroupStreams && ok; k++)
+        ok = cudaStreamCreateWithFlags(&b->gst[k], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&b->ev_join[k], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        lh_batch_destroy(b);
         return LH_ECUDA;
     }
     *out = b;
@@ -133,6 +143,12 @@ extern "C" int lh_batch_destroy(lh_batch *b)
     for (auto &s : b->slots)
         if (s) instance_free(*s);
     pool_release(b, 0);
+    for (int k = 0; k < lh_batch::kGroupStreams; k++) {
+        if (b->gst[k]) cudaStreamSynchronize(b->gst[k]);
+        if (b->gst[k]) cudaStreamDestroy(b->gst[k]);
+        if (b->ev_join[k]) cudaEventDestroy(b->ev_join[k]);
+    }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->st_up) cudaStreamDestroy(b->st_up);
     if (b->st) cudaStreamDestroy(b->st);
     delete b;
@@ -299,8 +315,24 @@ extern "C" int lh_batch_step(lh_batch *b, int nsteps)
     if (!b || nsteps < 0) return bfail(b, LH_EINVAL, "bad arguments");
     int rc = rebuild(b);
     if (rc) return rc;
-    for (int s = 0; s < nsteps; s++)
-        for (auto &g : b->groups) BCK(cudaGraphLaunch(g->gexec, b->st), "graph launch");
+    const int ng = (int)b->groups.size();
+    if (ng == 1) {
+        for (int s = 0; s < nsteps; s++) BCK(cudaGraphLaunch(b->groups[0]->gexec, b->st), "graph launch");
+        return LH_OK;
+    }
+    // group g on stream g % kGroupStreams, each stream's groups in order;
+    // every step forks from and joins back to the batch stream, so the
+    // batch stream orders steps, downloads and rebuilds as before
+    const int ns = std::min(ng, (int)lh_batch::kGroupStreams);
+    for (int s = 0; s < nsteps; s++) {
+        BCK(cudaEventRecord(b->ev_fork, b->st), "fork");
+        for (int k = 0; k < ns; k++) BCK(cudaStreamWaitEvent(b->gst[k], b->ev_fork, 0), "fork");
+        for (int g = 0; g < ng; g++) BCK(cudaGraphLaunch(b->groups[g]->gexec, b->gst[g % ns]), "graph launch");
+        for (int k = 0; k < ns; k++) {
+            BCK(cudaEventRecord(b->ev_join[k], b->gst[k]), "join");
+            BCK(cudaStreamWaitEvent(b->st, b->ev_join[k], 0), "join");
+        }
+    }
     return LH_OK;
 }
 
