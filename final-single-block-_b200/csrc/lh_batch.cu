@@ -250,9 +250,6 @@ extern "C" int lh_batch_remove(lh_batch *b, int slot)
 static int rebuild(lh_batch *b)
 {
     if (!b->dirty) return LH_OK;
-    // queued steps still read the plans and instance tables of groups that
-    // are freed below
-    BCK(cudaStreamSynchronize(b->st), "synchronize");
     const char *iso = getenv("LH_BATCH_ISOLATE");
     const long isolate = iso ? atol(iso) : kIsolateModes;
     // groups: the shared group of the smaller instances first, then one group
@@ -289,11 +286,14 @@ static int rebuild(lh_batch *b)
         cudaError_t e = cudaMalloc(&g->d_inst, hi.size() * sizeof(Inst));
         if (e == cudaSuccess) e = cudaMemcpy(g->d_inst, hi.data(), hi.size() * sizeof(Inst), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = plan_build(g->plan, v);
-        if (e == cudaSuccess) e = cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal);
+        // captured on the admission stream: the batch stream may still be
+        // running queued steps of the other groups
+        if (e == cudaSuccess) e = cudaStreamBeginCapture(b->st_up, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             cudaError_t el = cudaSuccess;
-            for (int kk = 1; kk <= 3 && el == cudaSuccess; kk++) el = launch_substep(g->plan, g->d_inst, kk, g->cfl, b->st);
-            cudaError_t ee = cudaStreamEndCapture(b->st, &g->graph);
+            for (int kk = 1; kk <= 3 && el == cudaSuccess; kk++)
+                el = launch_substep(g->plan, g->d_inst, kk, g->cfl, b->st_up);
+            cudaError_t ee = cudaStreamEndCapture(b->st_up, &g->graph);
             e = el != cudaSuccess ? el : ee;
         }
         if (e == cudaSuccess) e = cudaGraphInstantiate(&g->gexec, g->graph, 0);
@@ -303,6 +303,12 @@ static int rebuild(lh_batch *b)
         }
         next.push_back(std::move(g));
     }
+    // groups left without a match are freed; queued steps may still read
+    // their plans and instance tables, so only then wait for them (an
+    // admission that only adds groups keeps the device busy meanwhile)
+    bool stale = false;
+    for (auto &g : b->groups) stale |= (bool)g;
+    if (stale) BCK(cudaStreamSynchronize(b->st), "synchronize");
     for (auto &g : b->groups)
         if (g) free_group(*g);
     b->groups = std::move(next);
