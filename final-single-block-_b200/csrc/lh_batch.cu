@@ -10,9 +10,10 @@
 // staging share and splits their rounds, so each forms a launch group of its
 // own (its chunk rounds sized as if alone), while the smaller instances
 // share one group.  Every group keeps its own plan, instance table and CUDA
-// graph of one RK3 step; a batch step replays the groups' graphs on up to
-// four streams at once (forked from the batch stream and joined back), so a
-// large instance's latency-bound kernels overlap the others'.  When membership changes, only the groups
+// graph of one RK3 step; a batch step replays the groups' graphs one after
+// another on the batch stream (LH_BATCH_STREAMS = 2..4 replays them on that
+// many forked streams at once instead: measured slower on B200, the groups'
+// plane staging then competes for L2).  When membership changes, only the groups
 // whose members changed are planned and captured again -- an admission or a
 // retirement of a large instance leaves every other group's graph as it was.
 #include <cuda_runtime.h>
@@ -49,8 +50,8 @@ struct lh_batch {
     std::vector<std::unique_ptr<Group>> groups;
     cudaStream_t st = nullptr;
     cudaStream_t st_up = nullptr;  // admissions upload here while steps run on st
-    // the launch groups run concurrently on these streams, forked from st and
-    // joined back at every step (they touch disjoint instances)
+    // streams for replaying launch groups concurrently (LH_BATCH_STREAMS),
+    // forked from st and joined back at every step (disjoint instances)
     static constexpr int kGroupStreams = 4;
     cudaStream_t gst[kGroupStreams] = {};
     cudaEvent_t ev_fork = nullptr, ev_join[kGroupStreams] = {};
@@ -329,7 +330,13 @@ extern "C" int lh_batch_step(lh_batch *b, int nsteps)
     // group g on stream g % kGroupStreams, each stream's groups in order;
     // every step forks from and joins back to the batch stream, so the
     // batch stream orders steps, downloads and rebuilds as before
-    const int ns = std::min(ng, (int)lh_batch::kGroupStreams);
+    const char *gs = getenv("LH_BATCH_STREAMS");
+    const int ns = std::min(ng, std::max(1, std::min(gs ? atoi(gs) : 1, (int)lh_batch::kGroupStreams)));
+    if (ns == 1) {
+        for (int s = 0; s < nsteps; s++)
+            for (auto &g : b->groups) BCK(cudaGraphLaunch(g->gexec, b->st), "graph launch");
+        return LH_OK;
+    }
     for (int s = 0; s < nsteps; s++) {
         BCK(cudaEventRecord(b->ev_fork, b->st), "fork");
         for (int k = 0; k < ns; k++) BCK(cudaStreamWaitEvent(b->gst[k], b->ev_fork, 0), "fork");

@@ -5,7 +5,8 @@
 // the number of column-pass launches are chosen per (Mz, Mx, nyu) by timing
 // complete RK3 steps of a scratch instance of that size with CUDA events.
 // The search is coordinate descent from the built-in defaults: each
-// parameter in turn takes the best of a few candidates with the others held.
+// parameter in turn takes the best of a few candidates with the others held,
+// a candidate replacing the incumbent only when it is 2 % faster.
 // Nothing it varies changes any arithmetic -- every transform vector and
 // every column is computed by the same code whatever the tiling -- so a
 // tuned plan gives bit-identical states.
@@ -205,7 +206,9 @@ extern "C" int lh_autotune(lh_ctx *c, int force, int *params)
                 t.*(ax.first) = v;
                 double ms = 0.0;
                 e = trial(t, ms);
-                if (e == cudaSuccess && ms < best_ms) {
+                // a candidate must beat the incumbent by 2 %: run-to-run noise of
+                // a step is about 1-2 %, and an unchanged default is the safer pick
+                if (e == cudaSuccess && ms < 0.98 * best_ms) {
                     best_ms = ms;
                     best = t;
                 }
