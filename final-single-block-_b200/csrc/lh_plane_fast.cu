@@ -716,7 +716,10 @@ __global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_w(const Inst *__r
     constexpr int VT = N1 > N2 ? N1 : N2;
     if constexpr (32 % VT != 0) return;  // never launched (zfwd_warp_size)
     constexpr int LD = N2 + 1;
-    constexpr int REG = (NZ > N1 * LD ? NZ : N1 * LD);
+    // region stride rounded up to odd (in double2): the masks step reads the
+    // same z row of neighbouring modes' regions, which then fall in
+    // different banks
+    constexpr int REG = (NZ > N1 * LD ? NZ : N1 * LD) | 1;
     constexpr int Nz = 2 * NZ / 3;
     extern __shared__ double2 sm[];
     if ((int)blockIdx.x >= count) return;
@@ -927,7 +930,7 @@ size_t zfwd_smem(int n, int cb)
     switch (n) {
 #define LH_CASE(N)                                                                                  \
     case N: {                                                                                       \
-        const int reg = N > Plan2<N>::N1 * (Plan2<N>::N2 + 1) ? N : Plan2<N>::N1 * (Plan2<N>::N2 + 1); \
+        const int reg = (N > Plan2<N>::N1 * (Plan2<N>::N2 + 1) ? N : Plan2<N>::N1 * (Plan2<N>::N2 + 1)) | 1; \
         return (size_t)3 * cb * reg * sizeof(double2);                                            \
     }
         LH_FAST_SIZES(LH_CASE)
