@@ -52,8 +52,13 @@ class Request:
 
 
 def poisson_stream(n: int, rate: float, rng: np.random.Generator, grid_choices, ny_choices,
-                   retau=(100.0, 550.0), steps=(200, 5000), dt=(5e-4, 2e-3), base_seed: int = 20260005):
-    """Requests with Poisson arrivals, grids and Re_tau drawn as the serving config describes."""
+                   retau=(100.0, 550.0), steps=(200, 5000), dt=(5e-4, 2e-3), base_seed: int = 20260005,
+                   cfl: float | None = None):
+    """Requests with Poisson arrivals, grids and Re_tau drawn as the serving config describes.
+    With `cfl` every request runs in the reference's CFL mode at that number
+    (its input deck uses 0.7); otherwise a fixed dt drawn from `dt` -- which
+    at Re_tau 550 on the finest grids exceeds the convective limit and, over
+    thousands of steps, blows up."""
     t = 0.0
     out = []
     for k in range(n):
@@ -62,7 +67,11 @@ def poisson_stream(n: int, rate: float, rng: np.random.Generator, grid_choices, 
         ny = int(rng.choice(ny_choices))
         rt = float(rng.uniform(*retau))
         ns = int(round(math.exp(rng.uniform(math.log(steps[0]), math.log(steps[1])))))
-        d = Desc(Nx=N, Nz=N, ny=ny, Re=re_from_retau(rt), dt_mode=1, dt=float(rng.uniform(*dt)))
+        dtr = float(rng.uniform(*dt))
+        if cfl is None:
+            d = Desc(Nx=N, Nz=N, ny=ny, Re=re_from_retau(rt), dt_mode=1, dt=dtr)
+        else:
+            d = Desc(Nx=N, Nz=N, ny=ny, Re=re_from_retau(rt), dt_mode=0, CFL=cfl)
         out.append(Request(k, d, base_seed + 1000 * k, max(1, ns), t))
     return out
 
@@ -173,6 +182,8 @@ def serve(requests, hbm_budget: int, max_chunk: int = 50, keep_results: bool = T
                 tf = clock() - t0
                 for slot in finished:
                     r, _ = live.pop(slot)
+                    if hasattr(b, "scalars"):
+                        b.scalars(slot)  # raises if the instance's state became non-finite
                     if keep_results:
                         r.result = b.download(slot)
                     r.finished = tf
