@@ -29,7 +29,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .capi import Batch, Desc, Engine, LHError, LH_ENOMEM
+from .capi import Batch, Desc, Engine, LHError, LH_EDEVICE, LH_ENOMEM
 from .state import grids, perturbed_laminar, re_from_retau
 
 
@@ -44,6 +44,7 @@ class Request:
     admitted: float = math.nan
     finished: float = math.nan
     result: dict | None = None
+    error: str | None = None  # set when the simulation diverged (non-finite state)
 
     @property
     def work(self) -> float:
@@ -55,10 +56,13 @@ def poisson_stream(n: int, rate: float, rng: np.random.Generator, grid_choices, 
                    retau=(100.0, 550.0), steps=(200, 5000), dt=(5e-4, 2e-3), base_seed: int = 20260005,
                    cfl: float | None = None):
     """Requests with Poisson arrivals, grids and Re_tau drawn as the serving config describes.
-    With `cfl` every request runs in the reference's CFL mode at that number
-    (its input deck uses 0.7); otherwise a fixed dt drawn from `dt` -- which
-    at Re_tau 550 on the finest grids exceeds the convective limit and, over
-    thousands of steps, blows up."""
+    Every request runs at a fixed dt drawn from `dt`; with `cfl` it runs in
+    the reference's CFL mode at that number instead (its input deck uses 0.7).
+    The CFL rule sees only the x and z velocities (the reference never
+    assigns dthetavi, so its wall-normal term is infinite), and laminar
+    starts at Re_tau above ~400 run thousands of steps with a dt that breaks
+    the wall-normal limit: the oracle itself diverges on them even at CFL
+    0.25, while a fixed dt of 2e-4..5e-4 stays stable.""" 
     t = 0.0
     out = []
     for k in range(n):
@@ -183,8 +187,15 @@ def serve(requests, hbm_budget: int, max_chunk: int = 50, keep_results: bool = T
                 for slot in finished:
                     r, _ = live.pop(slot)
                     if hasattr(b, "scalars"):
-                        b.scalars(slot)  # raises if the instance's state became non-finite
-                    if keep_results:
+                        # a diverged simulation (non-finite state) is retired with
+                        # its error, as a server answers a failed request
+                        try:
+                            b.scalars(slot)
+                        except LHError as err:
+                            if err.code != LH_EDEVICE:
+                                raise
+                            r.error = "non-finite state"
+                    if keep_results and r.error is None:
                         r.result = b.download(slot)
                     r.finished = tf
                     b.remove(slot)
@@ -217,8 +228,13 @@ def run_plain(requests, keep_results: bool = True, clock=time.perf_counter, time
         e = Engine(r.desc)
         e.upload(*initial_state(r))
         e.step(r.nsteps)
-        e.synchronize()
-        if keep_results:
+        try:
+            e.synchronize()
+        except LHError as err:
+            if err.code != LH_EDEVICE:
+                raise
+            r.error = "non-finite state"
+        if keep_results and r.error is None:
             r.result = e.download()
         r.finished = clock() - t0
         e.close()
