@@ -43,6 +43,11 @@
 #ifndef LH_ZFWD_B
 #define LH_ZFWD_B 3
 #endif
+// iterations of the warp-local x stage's gather loop unrolled (its loads of
+// later modes are then issued before the shared-memory stores of earlier ones)
+#ifndef LH_XGATHER_UNROLL
+#define LH_XGATHER_UNROLL 1
+#endif
 #include "lh_kernels.cuh"
 
 namespace lh {
@@ -458,6 +463,8 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_w(const Inst *
         }
     };
     if (!DIRECT && live) {
+        constexpr int kGatherUnroll = LH_XGATHER_UNROLL;
+#pragma unroll kGatherUnroll
         for (int k = r; k < nxh; k += VT) {
             double2 A = make_double2(0.0, 0.0), B = A;
             if (rowok) rows_at(k, A, B);
