@@ -157,8 +157,23 @@ struct RowD {
     double g3, th;
 };
 
-__global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__restrict__ insts,
-                                                                const Work *__restrict__ work, int kRK)
+// Carried state of a forward-sweep chunk, per (role, column): u1/u3 roles
+// um, uc, flp, yp and the factor a3u; the u2 role um, uc, vvc, pc, yp and
+// a3v (the factor in .x of the last slot).
+constexpr int kCarryFields = 6;
+__device__ __forceinline__ double2 *carry_slot(const Inst &I, int role, int f, size_t col)
+{
+    return I.CARRY + ((size_t)role * kCarryFields + f) * I.nc + col;
+}
+
+// MODE 0: the whole pass in one launch (phase A writes the eliminated rows
+// in place into the state).  MODE 1: phase A only, for the u rows w.slot ..
+// w.blk of the work item (the u2 chain one row behind, since its y-flux
+// needs vv_c of the next plane), into the Y arrays, carrying the sweep's
+// state between chunks.  MODE 2: phases B-D, the back substitution reading
+// the Y arrays.
+template <int MODE>
+__device__ __forceinline__ void column_body(const Inst *__restrict__ insts, const Work *__restrict__ work, int kRK)
 {
     extern __shared__ double2 ring_mem[];
     const Work w = work[blockIdx.x];
@@ -198,28 +213,41 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
     using RingD = Ring<kRoles * kWarpSlots / 6, 6>;   // phase D (u1 warp, all slots)
 
     // ---------------- A: right-hand sides and forward elimination --------
-    if (live && role < 2) {
+    const int ja = MODE == 1 ? w.slot : 1, jb = MODE == 1 ? w.blk : nyu;  // u rows of this launch
+    if (MODE != 2 && live && role < 2) {
         // u1 (role 0) or u3 (role 1): RHS0_u1/u3 (littleharsh.f90:682-751,
         // 807-856), Nu sum (FOU3D.f90:268-281), du += -g Nu (:359-364),
         // solveU rhs (littleharsh.f90:878-890), LU_build/LU_dec on the fly;
         // both roles form the same u-grid factors with the same arithmetic.
         double2 *U = role == 0 ? U1 : U3;
+        double2 *YD = MODE == 0 ? U : (role == 0 ? I.Y1 : I.Y3) + cc;  // eliminated rows
         double2 *N = (role == 0 ? I.NU1 : I.NU3) + cc;
         const double2 *X = (role == 0 ? I.NXZ1 : I.NXZ3) + cc;
         const double2 *FL = (role == 0 ? I.UVF : I.WVF) + cc;
         // C3 = -dRK*k1F: (-0, -(d k)); C3*p = ((d k) p.im, -((d k) p.re))
         const double dC3 = rk.d * (role == 0 ? kxr : kzr);
         const double C1m = (role == 0 && mean) ? -rk.d * I.sc[SC_MPGX] : 0.0;
-        double2 um = U[0], uc = U[(size_t)nc];
-        double2 flp = FL[0];
-        double a3u = I.gw1 * 1.0;
-        double2 yp = make_double2(0.0, 0.0);
-        U[0] = yp;
-        if (role == 0) FU[0] = a3u;
+        double2 um, uc, flp, yp;
+        double a3u;
+        if (ja == 1) {
+            um = U[0];
+            uc = U[(size_t)nc];
+            flp = FL[0];
+            a3u = I.gw1 * 1.0;
+            yp = make_double2(0.0, 0.0);
+            YD[0] = yp;
+            if (role == 0) FU[0] = a3u;
+        } else {
+            um = *carry_slot(I, role, 0, cc);
+            uc = *carry_slot(I, role, 1, cc);
+            flp = *carry_slot(I, role, 2, cc);
+            yp = *carry_slot(I, role, 3, cc);
+            a3u = carry_slot(I, role, 4, cc)->x;
+        }
         const RingA ring{warp_mem, lane};
-        stream_rows<RingA::kDepth, 2>(nyu,
+        stream_rows<RingA::kDepth, 2>(jb - ja + 1,
                     [&](int r, int st) {
-                        const int j = r + 1;
+                        const int j = r + ja;
                         const size_t o = (size_t)j * nc, on = o - nc;
                         cp16(ring.at(st, 0), U + o + nc);
                         cp16(ring.at(st, 1), P + on);
@@ -228,12 +256,12 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         cp16(ring.at(st, 4), FL + o);
                     },
                     [&](int r, int st) {
-                        const int j = r + 1;
+                        const int j = r + ja;
                         return RowA{*ring.at(st, 0), *ring.at(st, 1), *ring.at(st, 2), *ring.at(st, 3), *ring.at(st, 4),
                                     du[3 * j], du[3 * j + 1], du[3 * j + 2], sthu[j]};
                     },
                     [&](int r, const RowA &w) {
-                        const int j = r + 1;
+                        const int j = r + ja;
                         const size_t o = (size_t)j * nc, on = o - nc;
                         const double2 up = w.a, pj = w.b, x = w.d, fl = w.e;
                         const double2 no = kRK == 1 ? make_double2(0.0, 0.0) : w.c;
@@ -253,33 +281,55 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         const double inv = 1.0 / (a2 - a1 * a3u);
                         const double2 y = make_double2((rh.x - a1 * yp.x) * inv, (rh.y - a1 * yp.y) * inv);
                         a3u = a3 * inv;
-                        U[o] = y;
+                        YD[o] = y;
                         if (role == 0) FU[o] = a3u;
                         yp = y;
                         um = uc;
                         uc = up;
                         flp = fl;
                     });
-        // top row: a = [gw2, 1, 0], rhs = 0
-        const double inv = 1.0 / (1.0 - I.gw2 * a3u);
-        U[(size_t)(nyu + 1) * nc] = make_double2((0.0 - I.gw2 * yp.x) * inv, (0.0 - I.gw2 * yp.y) * inv);
-    } else if (live && role == 2) {
+        if (jb == nyu) {
+            // top row: a = [gw2, 1, 0], rhs = 0
+            const double inv = 1.0 / (1.0 - I.gw2 * a3u);
+            YD[(size_t)(nyu + 1) * nc] = make_double2((0.0 - I.gw2 * yp.x) * inv, (0.0 - I.gw2 * yp.y) * inv);
+        } else {
+            *carry_slot(I, role, 0, cc) = um;
+            *carry_slot(I, role, 1, cc) = uc;
+            *carry_slot(I, role, 2, cc) = flp;
+            *carry_slot(I, role, 3, cc) = yp;
+            *carry_slot(I, role, 4, cc) = make_double2(a3u, 0.0);
+        }
+    } else if (MODE != 2 && live && role == 2) {
         // u2: RHS0_u2 (littleharsh.f90:753-805) with laplacian_V, Nu2 sum,
-        // solveU on the v grid
+        // solveU on the v grid; rows ja2 .. jb2 (one behind the u rows)
+        const int ja2 = MODE == 1 ? max(1, ja - 1) : 1, jb2 = MODE == 1 ? jb - 1 : nyv;
+        double2 *YD = MODE == 0 ? U2 : I.Y2 + cc;
         double2 *N = I.NU2 + cc;
         const double2 *X = I.NXZ2 + cc;
         const double2 *VV = I.VVC + cc;
-        double2 um = U2[0], uc = U2[(size_t)nc];
-        double2 vvc = VV[(size_t)nc];
-        double2 pc = P[0];
-        double a3v = 0.0 * 1.0;
-        double2 yp = make_double2(0.0, 0.0);
-        U2[0] = yp;
-        FV[0] = a3v;
+        double2 um, uc, vvc, pc, yp;
+        double a3v;
+        if (ja2 == 1) {
+            um = U2[0];
+            uc = U2[(size_t)nc];
+            vvc = VV[(size_t)nc];
+            pc = P[0];
+            a3v = 0.0 * 1.0;
+            yp = make_double2(0.0, 0.0);
+            YD[0] = yp;
+            FV[0] = a3v;
+        } else {
+            um = *carry_slot(I, 2, 0, cc);
+            uc = *carry_slot(I, 2, 1, cc);
+            vvc = *carry_slot(I, 2, 2, cc);
+            pc = *carry_slot(I, 2, 3, cc);
+            yp = *carry_slot(I, 2, 4, cc);
+            a3v = carry_slot(I, 2, 5, cc)->x;
+        }
         const RingA ring{warp_mem, lane};
-        stream_rows<RingA::kDepth, 2>(nyv,
+        stream_rows<RingA::kDepth, 2>(max(0, jb2 - ja2 + 1),
                     [&](int r, int st) {
-                        const int j = r + 1;
+                        const int j = r + ja2;
                         const size_t o = (size_t)j * nc, on = o - nc;
                         cp16(ring.at(st, 0), U2 + o + nc);
                         cp16(ring.at(st, 1), P + o);  // p(j+1)
@@ -288,12 +338,12 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         cp16(ring.at(st, 4), VV + o + nc);
                     },
                     [&](int r, int st) {
-                        const int j = r + 1;
+                        const int j = r + ja2;
                         return RowA{*ring.at(st, 0), *ring.at(st, 1), *ring.at(st, 2), *ring.at(st, 3), *ring.at(st, 4),
                                     dv[3 * j], dv[3 * j + 1], dv[3 * j + 2], sthv[j]};
                     },
                     [&](int r, const RowA &w) {
-                        const int j = r + 1;
+                        const int j = r + ja2;
                         const size_t o = (size_t)j * nc, on = o - nc;
                         const double2 up = w.a, pn = w.b, x = w.d, vvn = w.e;
                         const double2 no = kRK == 1 ? make_double2(0.0, 0.0) : w.c;
@@ -313,7 +363,7 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         const double inv = 1.0 / (b2 - b1 * a3v);
                         const double2 y = make_double2((rh.x - b1 * yp.x) * inv, (rh.y - b1 * yp.y) * inv);
                         a3v = b3 * inv;
-                        U2[o] = y;
+                        YD[o] = y;
                         FV[o] = a3v;
                         yp = y;
                         um = uc;
@@ -321,22 +371,35 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
                         vvc = vvn;
                         pc = pn;
                     });
-        const double inv = 1.0 / (1.0 - 0.0 * a3v);
-        U2[(size_t)(nyv + 1) * nc] = make_double2((0.0 - 0.0 * yp.x) * inv, (0.0 - 0.0 * yp.y) * inv);
+        if (jb2 == nyv) {
+            const double inv = 1.0 / (1.0 - 0.0 * a3v);
+            YD[(size_t)(nyv + 1) * nc] = make_double2((0.0 - 0.0 * yp.x) * inv, (0.0 - 0.0 * yp.y) * inv);
+        } else {
+            *carry_slot(I, 2, 0, cc) = um;
+            *carry_slot(I, 2, 1, cc) = uc;
+            *carry_slot(I, 2, 2, cc) = vvc;
+            *carry_slot(I, 2, 3, cc) = pc;
+            *carry_slot(I, 2, 4, cc) = yp;
+            *carry_slot(I, 2, 5, cc) = make_double2(a3v, 0.0);
+        }
     }
-    __syncthreads();
+    if (MODE == 1) return;
+    if (MODE == 0) __syncthreads();
 
     // ---------------- B: back substitution (tridLU_3D.f90:80-82) ----------
     if (live) {
         double2 *U = role == 0 ? U1 : (role == 1 ? U3 : U2);
+        // the eliminated rows: in place (MODE 0) or in the Y arrays (MODE 2)
+        const double2 *YS = MODE == 0 ? U : (role == 0 ? I.Y1 : (role == 1 ? I.Y3 : I.Y2)) + cc;
         const double *F = role == 2 ? FV : FU;
         const int top = role == 2 ? nyv + 1 : nyu + 1;
-        double2 v = U[(size_t)top * nc];
+        double2 v = YS[(size_t)top * nc];
+        if (MODE == 2) U[(size_t)top * nc] = v;
         const RingW2 ring{warp_mem, lane};
         stream_rows<RingW2::kDepth, 4>(top,
                     [&](int r, int st) {
                         const int j = top - 1 - r;
-                        cp16(ring.at(st, 0), U + (size_t)j * nc);
+                        cp16(ring.at(st, 0), YS + (size_t)j * nc);
                         cp8(&ring.at(st, 1)->x, F + (size_t)j * nc);
                     },
                     [&](int r, int st) { return RowB{*ring.at(st, 0), ring.at(st, 1)->x}; },
@@ -508,6 +571,24 @@ __global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__re
             I.sc[SC_ITER] = I.sc[SC_ITER] + 1.0;
         }
     }
+}
+
+__global__ void __launch_bounds__(kColThreads *kRoles) k_column(const Inst *__restrict__ insts,
+                                                                const Work *__restrict__ work, int kRK)
+{
+    column_body<0>(insts, work, kRK);
+}
+
+__global__ void __launch_bounds__(kColThreads *kRoles) k_column_a(const Inst *__restrict__ insts,
+                                                                  const Work *__restrict__ work, int kRK)
+{
+    column_body<1>(insts, work, kRK);
+}
+
+__global__ void __launch_bounds__(kColThreads *kRoles) k_column_bcd(const Inst *__restrict__ insts,
+                                                                    const Work *__restrict__ work, int kRK)
+{
+    column_body<2>(insts, work, kRK);
 }
 
 // ---------------------------------------------------------------------------

@@ -72,6 +72,8 @@ struct Inst {
     double2 *UVF, *WVF, *VVC;                 // y-flux spectra, rows 0..nyu(+1)
     double *FACU, *FACV;                      // scaled upper diagonals
     double2 *PSI;                             // pressure correction, rows 1..nyu
+    double2 *Y1, *Y2, *Y3;                    // forward-eliminated rows of a split column pass
+    double2 *CARRY;                           // sweep state between its chunks [3][6][nc]
     double *U11, *F11;                        // (0,0)-mode flow-rate solve, rows 0..nyu+1
     double2 *S;                               // plane-pipeline staging
     double *sc;                               // Scalar slots

@@ -109,6 +109,10 @@ void carve(const HostSetup &s, int chunk, Carver &c, Inst &I, double2 **stage, s
     I.FACU = c.take<double>(nu * nc);
     I.FACV = c.take<double>(nv * nc);
     I.PSI = c.take<double2>(np * nc);
+    I.Y1 = c.take<double2>(nu * nc);
+    I.Y2 = c.take<double2>(nv * nc);
+    I.Y3 = c.take<double2>(nu * nc);
+    I.CARRY = c.take<double2>(18 * nc);
     I.U11 = c.take<double>(nu);
     I.F11 = c.take<double>(nu);
     I.S = c.take<double2>(staging_units(chunk) * s.Mz * s.nxh);
@@ -268,6 +272,10 @@ cudaError_t instance_download(DevInstance &d, double *u1, double *u2, double *u3
     if (p && (e = download_field(d, I.P, s.nyu, p, st)) != cudaSuccess) return e;
     return cudaStreamSynchronize(st);
 }
+
+// Whether the sequential column pass is split into forward-sweep chunks
+// beside the plane rounds (LH_COLUMN_SPLIT=0/1 overrides).
+constexpr bool kColumnSplitDefault = false;
 
 // Plans with at most this many columns in all use the one-CTA-per-column
 // column pass (LH_SMALL_COLUMNS overrides).
@@ -518,7 +526,42 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
             }
     p.off_column = all.size();
     all.insert(all.end(), p.column.begin(), p.column.end());
+    // split column pass: per round, every instance's rows of that round x its
+    // column blocks; plus one chunk of all rows
+    const char *cs = getenv("LH_COLUMN_SPLIT");
+    p.col_split = !p.col_small && (cs ? cs[0] == '1' : kColumnSplitDefault);
+    p.col_a.assign(rounds, {0, 0});
+    p.off_col_full = p.n_col_full = 0;
+    if (p.col_split) {
+        for (int r = 0; r < rounds; r++) {
+            p.col_a[r].first = all.size();
+            for (int q = 0; q < (int)insts.size(); q++) {
+                const HostSetup &s = insts[q]->hs;
+                const int j0 = 1 + r * chunk_eff[q];
+                if (j0 > s.nyu) continue;
+                const int j1 = std::min(s.nyu, j0 + chunk_eff[q] - 1);
+                for (int b = 0; b < (s.nc + kColumnThreads - 1) / kColumnThreads; b++) all.push_back({q, b, j0, j1, 0});
+            }
+            p.col_a[r].second = all.size() - p.col_a[r].first;
+        }
+        p.off_col_full = all.size();
+        for (int q = 0; q < (int)insts.size(); q++) {
+            const HostSetup &s = insts[q]->hs;
+            for (int b = 0; b < (s.nc + kColumnThreads - 1) / kColumnThreads; b++) all.push_back({q, b, 1, s.nyu, 0});
+        }
+        p.n_col_full = all.size() - p.off_col_full;
+    }
     cudaError_t e = cudaSuccess;
+    if (p.col_split) {
+        if (!p.side_a) e = cudaStreamCreateWithFlags(&p.side_a, cudaStreamNonBlocking);
+        if (e == cudaSuccess && !p.ev_a) e = cudaEventCreateWithFlags(&p.ev_a, cudaEventDisableTiming);
+        while (e == cudaSuccess && p.ev_round.size() < (size_t)rounds) {
+            cudaEvent_t ev = nullptr;
+            e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            if (e == cudaSuccess) p.ev_round.push_back(ev);
+        }
+        if (e != cudaSuccess) return e;
+    }
     if (!p.ev_fork) e = cudaEventCreateWithFlags(&p.ev_fork, cudaEventDisableTiming);
     for (int k = 0; k < kRoundStreams - 1 && e == cudaSuccess; k++) {
         if (!p.side[k]) e = cudaStreamCreateWithFlags(&p.side[k], cudaStreamNonBlocking);
@@ -561,6 +604,8 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
         return raise_smem_limit((const void *)k_column_small, p.sm_col);
     }
     p.sm_col = column_smem_bytes(max_nyu);
+    if ((e = raise_smem_limit((const void *)k_column_a, p.sm_col)) != cudaSuccess) return e;
+    if ((e = raise_smem_limit((const void *)k_column_bcd, p.sm_col)) != cudaSuccess) return e;
     return raise_smem_limit((const void *)k_column, p.sm_col);
 }
 
@@ -578,6 +623,12 @@ void plan_free(Plan &p)
         p.side[k] = nullptr;
     }
     p.rounds.clear();
+    for (cudaEvent_t ev : p.ev_round) cudaEventDestroy(ev);
+    p.ev_round.clear();
+    if (p.ev_a) cudaEventDestroy(p.ev_a);
+    p.ev_a = nullptr;
+    if (p.side_a) cudaStreamDestroy(p.side_a);
+    p.side_a = nullptr;
 }
 
 static void time_begin(LaunchTimer *t, cudaStream_t st)
@@ -613,7 +664,15 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
         for (int k = 0; k < nstreams - 1; k++)
             if ((e = cudaStreamWaitEvent(p.side[k], p.ev_fork, 0)) != cudaSuccess) return e;
     }
-    for (size_t ri = 0; ri < p.rounds.size(); ri++)
+    // forward-sweep chunks beside the plane rounds (split column pass; not
+    // when dt is only known after the plane pass, nor in timed profiles)
+    const bool a_beside = p.col_split && !(kRK == 1 && cfl_any);
+    const bool a_stream = a_beside && timer == nullptr && p.side_a != nullptr;
+    if (a_stream) {
+        if (nstreams <= 1 && (e = cudaEventRecord(p.ev_fork, st)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(p.side_a, p.ev_fork, 0)) != cudaSuccess) return e;
+    }
+    for (size_t ri = 0; ri < p.rounds.size(); ri++) {
         for (const Group &g : p.rounds[ri]) {
             const Work *w = p.d_work + g.off;
             const unsigned n = (unsigned)g.count;
@@ -634,6 +693,25 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
             }
             if ((e = time_end(timer, g.stage, st)) != cudaSuccess) return e;
         }
+        if (a_beside && p.col_a[ri].second) {
+            const int si = (int)(ri % kRoundStreams);
+            cudaStream_t rs = (nstreams > 1 && si > 0) ? p.side[si - 1] : st;
+            cudaStream_t as = rs;
+            if (a_stream) {
+                if ((e = cudaEventRecord(p.ev_round[ri], rs)) != cudaSuccess) return e;
+                if ((e = cudaStreamWaitEvent(p.side_a, p.ev_round[ri], 0)) != cudaSuccess) return e;
+                as = p.side_a;
+            }
+            time_begin(timer, as);
+            k_column_a<<<(unsigned)p.col_a[ri].second, kColumnBlock, p.sm_col, as>>>(
+                d_insts, p.d_work + p.col_a[ri].first, kRK);
+            if ((e = time_end(timer, 4, as)) != cudaSuccess) return e;
+        }
+    }
+    if (a_stream) {
+        if ((e = cudaEventRecord(p.ev_a, p.side_a)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(st, p.ev_a, 0)) != cudaSuccess) return e;
+    }
     for (int k = 0; k < nstreams - 1; k++) {
         if ((e = cudaEventRecord(p.ev_join[k], p.side[k])) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(st, p.ev_join[k], 0)) != cudaSuccess) return e;
@@ -644,7 +722,11 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
         if ((e = time_end(timer, 3, st)) != cudaSuccess) return e;
     }
     time_begin(timer, st);
-    if (p.col_small)
+    if (p.col_split) {
+        if (!a_beside)
+            k_column_a<<<(unsigned)p.n_col_full, kColumnBlock, p.sm_col, st>>>(d_insts, p.d_work + p.off_col_full, kRK);
+        k_column_bcd<<<(unsigned)p.column.size(), kColumnBlock, p.sm_col, st>>>(d_insts, p.d_work + p.off_column, kRK);
+    } else if (p.col_small)
         k_column_small<<<(unsigned)p.column.size(), 32 * kSmallWarps, p.sm_col, st>>>(d_insts, p.d_work + p.off_column,
                                                                                       kRK);
     else {

@@ -97,6 +97,18 @@ struct Plan {
     size_t sm_col = 0;
     bool col_small = false;  // column pass by k_column_small (one CTA per column)
     int col_waves = 1;       // column-pass launches the column blocks are split over
+    // Split column pass (LH_COLUMN_SPLIT): its forward sweeps run in row
+    // chunks, one per plane round, on a stream of their own as soon as the
+    // round's z-forward is done, while later rounds still run; phases B-D
+    // follow in one launch.  Per round (offset, count) of the k_column_a work
+    // items, and a one-chunk list for substeps whose dt is only known after
+    // the plane pass (CFL mode, kRK = 1).
+    bool col_split = false;
+    std::vector<std::pair<size_t, size_t>> col_a;
+    size_t off_col_full = 0, n_col_full = 0;
+    cudaStream_t side_a = nullptr;
+    std::vector<cudaEvent_t> ev_round;
+    cudaEvent_t ev_a = nullptr;
     int ninst = 0;
     bool force_generic = false;
     cudaStream_t side[kRoundStreams - 1] = {};  // rounds r % kRoundStreams != 0

@@ -23,6 +23,9 @@ __global__ void k_plane_x_fwd(const Inst *__restrict__ insts, double *planes, in
 __global__ void k_plane_zero_row(const Inst *__restrict__ insts, double *planes);
 
 __global__ void k_column(const Inst *__restrict__ insts, const Work *__restrict__ work, int kRK);
+// the column pass split: forward sweeps in row chunks, then phases B-D
+__global__ void k_column_a(const Inst *__restrict__ insts, const Work *__restrict__ work, int kRK);
+__global__ void k_column_bcd(const Inst *__restrict__ insts, const Work *__restrict__ work, int kRK);
 __global__ void k_dt(const Inst *__restrict__ insts, int ninst);
 __global__ void k_col_to_plane(const double2 *__restrict__ src, double2 *__restrict__ dst, int len, int nc);
 __global__ void k_plane_to_col(const double2 *__restrict__ src, double2 *__restrict__ dst, int len, int nc);

@@ -374,3 +374,50 @@ def test_small_and_sequential_column_passes_agree(N, ctpress, ny, monkeypatch):
         assert rel_l2(out[0][0][f], out[1][0][f]) <= (1e-12 if f == "p" else 1e-13), f
     if ctpress == 0:
         assert abs(out[0][1]["mpgx"] - out[1][1]["mpgx"]) <= 1e-10 * abs(out[0][1]["mpgx"])
+
+
+@pytest.mark.parametrize("N,ny,ctpress,cfl", [(64, 97, 1, False), (128, 153, 1, False), (64, 65, 0, False),
+                                              (64, 97, 1, True)])
+def test_split_and_fused_column_passes_agree(N, ny, ctpress, cfl, monkeypatch):
+    """The column pass split into forward-sweep chunks (one per plane round,
+    run beside the later rounds, the sweep's state carried between chunks)
+    and phases B-D in one launch performs the same operations as the fused
+    pass, so the states agree bit for bit -- in CFL mode too, where the first
+    substep's forward sweep waits for the time step."""
+    from lh_b200 import Desc, grids, perturbed_laminar
+    monkeypatch.setenv("LH_SMALL_COLUMNS", "0")
+    d = Desc(Nx=N, Nz=N, ny=ny, flag_ctpress=ctpress, dt_mode=0 if cfl else 1, dt=5e-4, CFL=0.5)
+    ic = perturbed_laminar(d, 13, *grids(d))
+    out = []
+    for split in ("0", "1"):
+        monkeypatch.setenv("LH_COLUMN_SPLIT", split)
+        e = _engine(d)
+        e.upload(*ic)
+        e.step(3)
+        e.synchronize()
+        out.append((e.download(), e.scalars()))
+    for f in FIELDS:
+        assert np.array_equal(out[0][0][f], out[1][0][f]), f
+    assert out[0][1] == out[1][1]
+
+
+def test_split_column_pass_in_a_batch(monkeypatch):
+    """Forward-sweep chunks of a batch cover each instance's own rounds (the
+    instances' chunk sizes differ); every instance ends as with the fused pass."""
+    from lh_b200 import Batch, Desc, grids, perturbed_laminar
+    monkeypatch.setenv("LH_SMALL_COLUMNS", "0")
+    descs = [Desc(Nx=64, Nz=64, ny=97, dt_mode=1, dt=5e-4), Desc(Nx=32, Nz=32, ny=153, dt_mode=1, dt=1e-3),
+             Desc(Nx=128, Nz=128, ny=153, dt_mode=0, CFL=0.5)]
+    ics = [perturbed_laminar(d, 40 + k, *grids(d)) for k, d in enumerate(descs)]
+    res = []
+    for split in ("0", "1"):
+        monkeypatch.setenv("LH_COLUMN_SPLIT", split)
+        b = Batch()
+        slots = [b.add(d, *ic) for d, ic in zip(descs, ics)]
+        b.step(2)
+        b.synchronize()
+        res.append([b.download(s) for s in slots])
+        b.close()
+    for a, c in zip(res[0], res[1]):
+        for f in FIELDS:
+            assert np.array_equal(a[f], c[f]), f
