@@ -59,7 +59,10 @@ constexpr int kRoles = kColumnBlock / kColumnThreads;
 // Row slots (one complex per lane, 512 B per warp) of shared memory each
 // warp owns; a phase that loads S slots per row keeps kWarpSlots / S rows in
 // flight, and the single-warp Poisson sweeps use all warps' slots.
-constexpr int kWarpSlots = 40;
+#ifndef LH_COLUMN_SLOTS
+#define LH_COLUMN_SLOTS 40
+#endif
+constexpr int kWarpSlots = LH_COLUMN_SLOTS;
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void cp16(double2 *s, const double2 *g)
