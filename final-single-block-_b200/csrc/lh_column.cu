@@ -73,6 +73,62 @@ __device__ __forceinline__ void cp8(double *s, const double *g)
 {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(s)), "l"(g));
 }
+// L2 eviction hints (LH_COLUMN_HINTS, compile time; 0 = none): 1 marks the
+// forward sweep's read-once rows (Nu_old, the Nu x/z parts, the y fluxes)
+// and the Nu and psi rows no later sweep of the launch reads as evict-first;
+// 2 also marks the rows the later sweeps read back (eliminated rows, factors,
+// the forward Poisson sweep) as evict-last.
+#ifndef LH_COLUMN_HINTS
+#define LH_COLUMN_HINTS 0
+#endif
+struct Hints {
+    unsigned long long first, last;
+    __device__ Hints()
+    {
+        first = last = 0ull;
+#if LH_COLUMN_HINTS >= 1
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(first));
+#endif
+#if LH_COLUMN_HINTS >= 2
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(last));
+#endif
+    }
+    __device__ __forceinline__ void cp_once(double2 *s, const double2 *g) const
+    {
+#if LH_COLUMN_HINTS >= 1
+        asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(smem_addr(s)), "l"(g),
+                     "l"(first));
+#else
+        cp16(s, g);
+#endif
+    }
+    __device__ __forceinline__ void st_once(double2 *g, double2 v) const
+    {
+#if LH_COLUMN_HINTS >= 1
+        asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(g), "d"(v.x), "d"(v.y), "l"(first)
+                     : "memory");
+#else
+        *g = v;
+#endif
+    }
+    __device__ __forceinline__ void st_back(double2 *g, double2 v) const
+    {
+#if LH_COLUMN_HINTS >= 2
+        asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(g), "d"(v.x), "d"(v.y), "l"(last)
+                     : "memory");
+#else
+        *g = v;
+#endif
+    }
+    __device__ __forceinline__ void st_back(double *g, double v) const
+    {
+#if LH_COLUMN_HINTS >= 2
+        asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(g), "d"(v), "l"(last) : "memory");
+#else
+        *g = v;
+#endif
+    }
+};
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait()
@@ -210,6 +266,7 @@ __device__ __forceinline__ void column_body(const Inst *__restrict__ insts, cons
     __syncthreads();
     const double *du = sdu, *dv = sdv;
     double2 *warp_mem = ring_mem + (size_t)role * kWarpSlots * kColThreads;
+    const Hints hint;
     using RingA = Ring<kWarpSlots / 5, 5>;         // phase A: 5 slots per row
     using RingW2 = Ring<kWarpSlots / 2, 2>;        // phase B: 2 slots per row
     using RingC = Ring<kRoles * kWarpSlots / 4, 4>;   // phase C (u1 warp, all slots)
@@ -254,9 +311,9 @@ __device__ __forceinline__ void column_body(const Inst *__restrict__ insts, cons
                         const size_t o = (size_t)j * nc, on = o - nc;
                         cp16(ring.at(st, 0), U + o + nc);
                         cp16(ring.at(st, 1), P + on);
-                        if (kRK != 1) cp16(ring.at(st, 2), N + on);  // c_1 = 0: Nu_old unused
-                        cp16(ring.at(st, 3), X + on);
-                        cp16(ring.at(st, 4), FL + o);
+                        if (kRK != 1) hint.cp_once(ring.at(st, 2), N + on);  // c_1 = 0: Nu_old unused
+                        hint.cp_once(ring.at(st, 3), X + on);
+                        hint.cp_once(ring.at(st, 4), FL + o);
                     },
                     [&](int r, int st) {
                         const int j = r + ja;
@@ -275,7 +332,7 @@ __device__ __forceinline__ void column_body(const Inst *__restrict__ insts, cons
                         if (role == 0 && mean) dd.x = dd.x + C1m;
                         const double m = w.m3;
                         const double2 nu = make_double2(x.x + (fl.x - flp.x) * m * ddv, x.y + (fl.y - flp.y) * m * ddv);
-                        N[on] = nu;
+                        hint.st_once(N + on, nu);
                         dd = make_double2(dd.x + G * nu.x, dd.y + G * nu.y);
                         const double2 rh = make_double2(uc.x + dt * dd.x, uc.y + dt * dd.y);
                         const double a1 = -beta * d1;
@@ -284,8 +341,8 @@ __device__ __forceinline__ void column_body(const Inst *__restrict__ insts, cons
                         const double inv = 1.0 / (a2 - a1 * a3u);
                         const double2 y = make_double2((rh.x - a1 * yp.x) * inv, (rh.y - a1 * yp.y) * inv);
                         a3u = a3 * inv;
-                        YD[o] = y;
-                        if (role == 0) FU[o] = a3u;
+                        hint.st_back(YD + o, y);
+                        if (role == 0) hint.st_back(FU + o, a3u);
                         yp = y;
                         um = uc;
                         uc = up;
@@ -336,9 +393,9 @@ __device__ __forceinline__ void column_body(const Inst *__restrict__ insts, cons
                         const size_t o = (size_t)j * nc, on = o - nc;
                         cp16(ring.at(st, 0), U2 + o + nc);
                         cp16(ring.at(st, 1), P + o);  // p(j+1)
-                        if (kRK != 1) cp16(ring.at(st, 2), N + on);  // c_1 = 0: Nu_old unused
-                        cp16(ring.at(st, 3), X + on);
-                        cp16(ring.at(st, 4), VV + o + nc);
+                        if (kRK != 1) hint.cp_once(ring.at(st, 2), N + on);  // c_1 = 0: Nu_old unused
+                        hint.cp_once(ring.at(st, 3), X + on);
+                        hint.cp_once(ring.at(st, 4), VV + o + nc);
                     },
                     [&](int r, int st) {
                         const int j = r + ja2;
@@ -357,7 +414,7 @@ __device__ __forceinline__ void column_body(const Inst *__restrict__ insts, cons
                         const double C3 = -rk.d * ddv * mv;
                         double2 dd = make_double2(C1 * L.x + C2 * no.x + C3 * (pn.x - pc.x), C1 * L.y + C2 * no.y + C3 * (pn.y - pc.y));
                         const double2 nu = make_double2(x.x + (vvn.x - vvc.x) * mv * ddv, x.y + (vvn.y - vvc.y) * mv * ddv);
-                        N[on] = nu;
+                        hint.st_once(N + on, nu);
                         dd = make_double2(dd.x + G * nu.x, dd.y + G * nu.y);
                         const double2 rh = make_double2(uc.x + dt * dd.x, uc.y + dt * dd.y);
                         const double b1 = -beta * e1;
@@ -366,8 +423,8 @@ __device__ __forceinline__ void column_body(const Inst *__restrict__ insts, cons
                         const double inv = 1.0 / (b2 - b1 * a3v);
                         const double2 y = make_double2((rh.x - b1 * yp.x) * inv, (rh.y - b1 * yp.y) * inv);
                         a3v = b3 * inv;
-                        YD[o] = y;
-                        FV[o] = a3v;
+                        hint.st_back(YD + o, y);
+                        hint.st_back(FV + o, a3v);
                         yp = y;
                         um = uc;
                         uc = up;
@@ -501,7 +558,7 @@ __device__ __forceinline__ void column_body(const Inst *__restrict__ insts, cons
                             const double g1 = w.g1;
                             xp = make_double2((ps.x - g1 * xp.x) * g2, (ps.y - g1 * xp.y) * g2);
                         }
-                        PS[(size_t)(j - 1) * nc] = xp;
+                        hint.st_back(PS + (size_t)(j - 1) * nc, xp);
                         v2m = v2c;
                     });
         // ---------------- D: LUsolP back sweep, p += psi and v_corr ---------
@@ -519,7 +576,7 @@ __device__ __forceinline__ void column_body(const Inst *__restrict__ insts, cons
                     [&](int r, int st) {
                         const int j = nyu - r;
                         const size_t o = (size_t)(j - 1) * nc, oj = (size_t)j * nc;
-                        cp16(ringd.at(st, 0), PS + o);
+                        hint.cp_once(ringd.at(st, 0), PS + o);
                         cp16(ringd.at(st, 1), P + o);
                         if (j < nyu) cp8(&ringd.at(st, 2)->x, G3 + o);
                         cp16(ringd.at(st, 3), U1 + oj);

@@ -25,6 +25,10 @@ constexpr int kNumProducts = 6;
 #define LH_ROUND_STREAMS 2
 #endif
 constexpr int kRoundStreams = LH_ROUND_STREAMS;
+// Planes per work item of the multi-plane x stage (odd, so that its v-row
+// pairs, which start at the group's first plane, cover the group exactly);
+// groups start at absolute planes 1 + kXGroup g.
+constexpr int kXGroup = 5;
 
 // Radix-3 constant exactly as the reference's FFTPACK carries it
 // (cft_buff.f:333, rft_buff.f:364): 15 significant digits.

@@ -310,7 +310,7 @@ ClassTiles fast_tiles(const HostSetup &s, int cbz_max, int rb, int cbf_max)
     c.smz = zinv_smem(s.Mz, c.cbz);
     rb = std::max(1, std::min(rb, s.Mz));
     // the x stage's vectors sit at an odd row stride (3 rb rounded up to odd)
-    while (rb > 1 && !(xprod_threads(s.Mx, rb) <= fast_max_threads(1) && xprod_smem(s.Mx, rb) <= smax)) rb--;
+    while (rb > 1 && !(xprod_threads(s.Mx, rb) <= xprod_max_threads(s.Mx) && xprod_smem(s.Mx, rb) <= smax)) rb--;
     c.rbx = rb;
     c.tx = xprod_threads(s.Mx, rb);
     c.smx = xprod_smem(s.Mx, rb);
@@ -335,7 +335,8 @@ void default_bounds(const HostSetup &s, int &cbz, int &rbx, int &cbf)
 {
     const int vz = std::max(1, fast_vector_threads(s.Mz)), vx = std::max(1, fast_vector_threads(s.Mx));
     cbz = 256 / vz;
-    rbx = std::max(1, 64 / vx);
+    // the multi-plane x stage holds seven vectors per z row: one row group
+    rbx = std::max(1, (xprod_multi(s.Mx) ? 32 : 64) / vx);
     cbf = std::max(1, 80 / vz - ((s.Mz == 96 || s.Mz == 192) ? 1 : 0));
 }
 
@@ -440,6 +441,9 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
         size_t c = fast ? (units > fixed ? (units - fixed) / 9 : kRoundStreams) : units / kNumProducts;
         c = std::max<size_t>(c / kRoundStreams, (size_t)(s.nyu + 7) / 8);
         c = std::max<size_t>(1, std::min<size_t>(c, (size_t)insts[q]->inst.chunk / kRoundStreams));
+        // the multi-plane x stage's groups start at absolute planes 1 + kXGroup g,
+        // so rounds hold whole groups
+        if (fast && xprod_multi(s.Mx) && c >= (size_t)kXGroup) c -= c % kXGroup;
         chunk_eff[q] = (int)c;
         rounds = std::max(rounds, (s.nyu + chunk_eff[q] - 1) / chunk_eff[q]);
     }
@@ -482,8 +486,15 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
                         for (int b = 0; b < nbz; b++)
                             L[0][cls_of[q]].push_back({q, jp, sb + jp - j0 + 1, f * nbz + b, 0});
                     }
+                if (xprod_multi(s.Mx))
+                    for (int j = j0; j <= j1; j += kXGroup) {
+                        const int np = std::min(kXGroup, j1 - j + 1);
+                        for (int b = 0; b < nbx; b++)
+                            L[1][cls_of[q]].push_back({q, j, pb + j - j0, b | (np << 16), sb + j - j0});
+                    }
                 for (int j = j0; j <= j1; j++) {
-                    for (int b = 0; b < nbx; b++) L[1][cls_of[q]].push_back({q, j, pb + j - j0, b, sb + j - j0});
+                    if (!xprod_multi(s.Mx))
+                        for (int b = 0; b < nbx; b++) L[1][cls_of[q]].push_back({q, j, pb + j - j0, b, sb + j - j0});
                     for (int b = 0; b < nbf; b++)
                         for (int h = 0; h < 2; h++) L[2][cls_of[q]].push_back({q, j, pb + j - j0, 2 * b + h, 0});
                 }

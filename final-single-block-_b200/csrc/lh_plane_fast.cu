@@ -37,6 +37,12 @@
 #ifndef LH_XPROD_B
 #define LH_XPROD_B 3
 #endif
+#ifndef LH_XMULTI_T
+#define LH_XMULTI_T 192
+#endif
+#ifndef LH_XMULTI_B
+#define LH_XMULTI_B 2
+#endif
 #ifndef LH_ZFWD_T
 #define LH_ZFWD_T 256
 #endif
@@ -616,6 +622,228 @@ __global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_w(const Inst *
     }
 }
 
+// Two-pass transform of one packed vector of length NX held by the VT lanes
+// of a warp in its shared-memory region z (natural order in and out; the
+// N1 x (N2 + 1) padded matrix in between).  SGN = +1 inverse, -1 forward.
+// Every lane of the warp calls it (act = false only joins the __syncwarp).
+template <int NX, int SGN>
+__device__ __forceinline__ void xvec_fft(double2 *z, const double2 *tw, double2 twr, int r, bool act)
+{
+    constexpr int N1 = Plan2<NX>::N1, N2 = Plan2<NX>::N2;
+    constexpr int LD = N2 + 1;
+    __syncwarp();
+    {
+        double2 a[N1];
+        if (act && r < N2) {
+#pragma unroll
+            for (int n1 = 0; n1 < N1; n1++) a[n1] = z[r + N2 * n1];
+        }
+        __syncwarp();
+        if (act && r < N2) {
+            DFT<N1, SGN, NX>::run(a, tw);
+            TwStep ts(twr);
+#pragma unroll
+            for (int k1 = 0; k1 < N1; k1++) {
+                double2 y = a[k1];
+                if (k1 > 0) y = twiddle<SGN>(ts.next(), y);
+                z[k1 * LD + r] = y;
+            }
+        }
+    }
+    __syncwarp();
+    {
+        double2 b[N2];
+        if (act && r < N1) {
+#pragma unroll
+            for (int n2 = 0; n2 < N2; n2++) b[n2] = z[r * LD + n2];
+            DFT<N2, SGN, NX>::run(b, tw);
+        }
+        __syncwarp();
+        if (act && r < N1) {
+#pragma unroll
+            for (int k2 = 0; k2 < N2; k2++) z[r + N1 * k2] = b[k2];
+        }
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// The x stage over a group of consecutive planes (the default where a
+// vector fits a warp).  The y interpolations are linear and commute with
+// the x transform too, so this stage transforms each y row's fields once --
+// (u1, u3) of a u plane as one packed vector, two adjacent v rows as
+// another -- and interpolates the physical rows of neighbouring planes: u2
+// at the u plane (interp_v, FOU3D.f90:407), u1 and u3 at the v plane
+// (interp_u, :387), with the weights of k_xprod_w.  Per plane that is 1.5
+// inverse transforms instead of 3, and 3 staging rows read instead of 8.
+//
+// A work item is a group of np <= kXGroup planes j .. j+np-1 and a block of
+// rb z rows; the plan starts groups at absolute planes 1 + kXGroup g, and v
+// rows are paired from the group's first plane, V_m = (v(j-1+2m), v(j+2m)),
+// so every row is transformed with the same partner -- and every plane's
+// products come out of the same operations -- whatever the plan's rounds,
+// staging budget or batch, as long as a round holds at least kXGroup planes
+// (below that the groups are cut at the round boundaries).  A row's physical
+// values depend on the partner packed with it at the rounding level.
+//
+// Each z row runs sub-rounds of three vectors on its three vector slots
+// (VT lanes each, one warp-local transform per vector): sub-round 0
+// transforms A_0 = (u1, u3)(j), A_1 and V_0, after which plane j's products
+// are formed and transformed forward; sub-round k >= 1 transforms A_2k,
+// A_2k+1 and V_k, after which planes j+2k-1 and j+2k follow.  Regions per z
+// row: three for the A vectors (index mod 3), two for the V vectors (mod 2)
+// and two for the second and third product pairs; the first pair (u1 u1,
+// u1 u3) overwrites A_p in place.  Row groups of 96 threads synchronise on a
+// named barrier of their own before each sub-round and around each plane's
+// products.  Same transforms, products, split and CFL maxima as k_xprod_w.
+template <int NX>
+__global__ void __launch_bounds__(LH_XMULTI_T, LH_XMULTI_B) k_xprod_m(const Inst *__restrict__ insts,
+                                                                      const Work *__restrict__ work, int count,
+                                                                      int rb, int want_max)
+{
+    constexpr int N1 = Plan2<NX>::N1, N2 = Plan2<NX>::N2;
+    constexpr int VT = N1 > N2 ? N1 : N2;
+    if constexpr (32 % VT != 0) return;  // never launched (xprod_warp_size)
+    constexpr int LD = N2 + 1;
+    constexpr int REG = (NX > N1 * LD ? NX : N1 * LD);
+    constexpr int RG = 32 / VT;  // rows per 96-thread group
+    constexpr int nxh = NX / 3 + 1;
+    constexpr int kRegions = 7;
+    extern __shared__ double2 sm[];
+    if ((int)blockIdx.x >= count) return;
+    const double2 *tw = insts[work[blockIdx.x].inst].twx;
+    const int t = threadIdx.x, v = t / VT, r = t % VT;
+    const int row = v / 3, slot = v % 3, grp = row / RG;
+    const double2 twr = __ldg(tw + (r < N2 ? r : 0));
+    const Work w = work[blockIdx.x];
+    const Inst &I = insts[w.inst];
+    const int Mz = I.Mz, j = w.j, np = w.blk >> 16;
+    const int q = (w.blk & 0xffff) * rb + row;  // this thread's z row
+    const bool live = row < rb;                  // threads past the CTA's rows only join the barriers
+    const bool rowok = live && q < Mz;
+    double2 *const R = sm + (size_t)(live ? row : 0) * kRegions * REG;
+    const size_t fs = (size_t)Mz * nxh, orow = (size_t)q * nxh;
+    const bool track = want_max && I.dt_mode == 0;
+    double m1 = 0.0, m3 = 0.0;
+    // sub-round k: the inverse transforms of A_2k, A_2k+1 and V_k
+    auto subround = [&](const int k) {
+        // the regions this sub-round fills were last read by other slots
+        if (k > 0) asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(96) : "memory");
+        double2 *z;
+        const double2 *sa = nullptr, *sb = nullptr;
+        bool act = live;
+        if (slot < 2) {
+            const int tt = 2 * k + slot;  // A_tt: (u1, u3) of plane j + tt
+            z = R + (tt % 3) * REG;
+            act = act && tt <= np;
+            sa = sin_field(I, w.aux + 1 + tt, 0);
+            sb = sa + fs;
+        } else {
+            // V_k: v rows j-1+2k and j+2k; the second is past the group only
+            // when np is even, i.e. in the last group below the top wall,
+            // where it is the ghost row above v(nyu): zero
+            z = R + (3 + (k & 1)) * REG;
+            sa = sin_field(I, w.aux + 2 * k, 2);
+            sb = 2 * k < np ? sin_field(I, w.aux + 2 * k + 1, 2) : nullptr;
+        }
+        if (act) {
+            for (int m = r; m < nxh; m += VT) {
+                double2 A = make_double2(0.0, 0.0), B = A;
+                if (rowok) {
+                    A = sa[orow + m];
+                    if (sb) B = sb[orow + m];
+                }
+                if (m == 0) {
+                    z[0] = make_double2(A.x, B.x);
+                } else {
+                    z[m] = make_double2(A.x - B.y, A.y + B.x);
+                    z[NX - m] = make_double2(A.x + B.y, B.x - A.y);
+                }
+            }
+            for (int x = nxh + r; x <= NX - nxh; x += VT) z[x] = make_double2(0.0, 0.0);
+        }
+        xvec_fft<NX, +1>(z, tw, twr, r, act);
+    };
+    // plane j + p: products, forward transforms and split
+    auto plane = [&](const int p) {
+        const int jp = j + p;
+        const double dnv = 1.0 / (I.yv[jp] - I.yv[jp - 1]), dnu = 1.0 / (I.yu[jp + 1] - I.yu[jp]);
+        const double w0v = (I.yu[jp] - I.yv[jp - 1]) * dnv, w1v = (I.yv[jp] - I.yu[jp]) * dnv;
+        const double w0u = (I.yv[jp] - I.yu[jp]) * dnu, w1u = (I.yu[jp + 1] - I.yv[jp]) * dnu;
+        const bool trk = track && jp <= I.nyu - 1;
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(96) : "memory");
+        {
+            const int gt = t - grp * 96, row0 = grp * RG;
+            const int ra = p % 3, rn = (p + 1) % 3, rvm = 3 + ((p >> 1) & 1), rvv = 3 + (((p + 1) >> 1) & 1);
+            for (int e = gt; e < RG * NX; e += 96) {
+                const int rr = row0 + e / NX, x = e % NX;
+                if (rr >= rb) continue;
+                double2 *Rr = sm + (size_t)rr * kRegions * REG;
+                const double2 a0 = Rr[ra * REG + x], a1 = Rr[rn * REG + x];
+                const double2 c0 = Rr[rvm * REG + x], c1 = Rr[rvv * REG + x];
+                const double u1 = a0.x, u3 = a0.y;
+                const double vm = (p & 1) ? c0.y : c0.x;        // v(jp - 1)
+                const double u2 = ((p + 1) & 1) ? c1.y : c1.x;  // v(jp)
+                const double u2c = w0v * u2 + w1v * vm;
+                const double u1f = w0u * a1.x + w1u * u1, u3f = w0u * a1.y + w1u * u3;
+                if (trk && (w.blk & 0xffff) * rb + rr < Mz) {
+                    m1 = fmax(m1, fabs(u1));
+                    m3 = fmax(m3, fabs(u3));
+                }
+                Rr[ra * REG + x] = make_double2(u1 * u1, u1 * u3);
+                Rr[5 * REG + x] = make_double2(u2c * u2c, u3 * u3);
+                Rr[6 * REG + x] = make_double2(u1f * u2, u3f * u2);
+            }
+        }
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(96) : "memory");
+        double2 *zf = R + (slot == 0 ? p % 3 : 4 + slot) * REG;
+        xvec_fft<NX, -1>(zf, tw, twr, r, live);
+        // split the packed real transforms, scale 1/Mx, keep modes i <= Nx/2
+        if (rowok) {
+            double2 *S = sprod_slot(I, w.slot + p);
+            const double dn1 = 1.0 / NX;
+            for (int m = r; m < nxh; m += VT) {
+                const double2 zk = zf[m];
+                const double2 zm = zf[m == 0 ? 0 : NX - m];
+                double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+                double2 B = make_double2(0.5 * (zk.y + zm.y), 0.5 * (zm.x - zk.x));
+                if (m == 0) {
+                    A.y = 0.0;
+                    B.y = 0.0;
+                }
+                S[((size_t)(2 * slot) * Mz + q) * nxh + m] = make_double2(dn1 * A.x, dn1 * A.y);
+                S[((size_t)(2 * slot + 1) * Mz + q) * nxh + m] = make_double2(dn1 * B.x, dn1 * B.y);
+            }
+        }
+    };
+    // straight-line code for the group size: as a runtime loop over the
+    // sub-rounds the compiler keeps values live across iterations and spills
+    // (168 registers and 1.3 KB of spills at Mx = 192, against 124 and none)
+    static_assert(kXGroup == 5, "the sequence below covers groups of five planes");
+    subround(0);
+    plane(0);
+    if (np > 1) {
+        subround(1);
+        plane(1);
+        if (np > 2) plane(2);
+    }
+    if (np > 3) {
+        subround(2);
+        plane(3);
+        if (np > 4) plane(4);
+    }
+    if (track) {
+        for (int o = 16; o > 0; o >>= 1) {
+            m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+            m3 = fmax(m3, __shfl_xor_sync(0xffffffffu, m3, o));
+        }
+        if ((t & 31) == 0) {
+            atomicMax(reinterpret_cast<unsigned long long *>(&I.sc[SC_U1MAX]), (unsigned long long)__double_as_longlong(m1));
+            atomicMax(reinterpret_cast<unsigned long long *>(&I.sc[SC_U3MAX]), (unsigned long long)__double_as_longlong(m3));
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // z forward, masks and derivatives of one (plane, block of cb x modes, half):
 // phys_to_four_du's cft (FOU3D.f90:1654-1672), der_x/der_z (:420-523) and
@@ -809,6 +1037,7 @@ __global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_w(const Inst *__r
 // ---------------------------------------------------------------------------
 // host dispatch
 int fast_max_threads(int stage) { return stage == 0 ? LH_ZINV_T : (stage == 1 ? LH_XPROD_T : LH_ZFWD_T); }
+int xprod_max_threads(int n) { return xprod_multi(n) ? LH_XMULTI_T : LH_XPROD_T; }
 
 bool fast_size(int n)
 {
@@ -875,24 +1104,26 @@ bool zinv_warp(int n)
     return ev && ev[0] == '1' && zinv_warp_size(n);
 }
 
-// x stage: sizes whose vectors fit a warp, and the variant selection
+// x stage: sizes whose vectors fit a warp, and the variant selection.
+// Where a vector fits a warp the warp-local k_xprod_w is the default
+// (measured on B200 at 128x128x153: x products 0.256 -> 0.236 ms per
+// substep, step 1.283 -> 1.218 ms); LH_XPROD_WARP selects the others for
+// measurement: 0 the block-synchronous k_xprod_f, 2 k_xprod_w's direct-read
+// form, 3 the multi-plane k_xprod_m.
 bool xprod_warp_size(int n) { return zinv_warp_size(n); }
-// The warp-local x stage is the default where it applies (measured on B200
-// at 128x128x153: x products 0.256 -> 0.236 ms per substep, step 1.283 ->
-// 1.218 ms); LH_XPROD_WARP=0 selects the block-synchronous kernel.
-bool xprod_warp(int n)
+static int xprod_mode(int n)
 {
+    if (!xprod_warp_size(n)) return 0;
     const char *ev = getenv("LH_XPROD_WARP");
-    return (!ev || ev[0] == '1' || ev[0] == '2') && xprod_warp_size(n);
+    if (!ev || !*ev || ev[0] == '1') return 1;
+    return ev[0] == '3' ? 3 : (ev[0] == '2' ? 2 : 0);
 }
-bool xprod_direct()
-{
-    const char *ev = getenv("LH_XPROD_WARP");
-    return ev && ev[0] == '2';
-}
+bool xprod_warp(int n) { return xprod_mode(n) != 0; }
+bool xprod_multi(int n) { return xprod_mode(n) == 3; }
 
-// Threads and shared memory of an x-stage CTA of rb z rows: the warp variant
-// runs 96-thread row groups (32 / VT rows each), one region per vector.
+// Threads and shared memory of an x-stage CTA of rb z rows: the warp variants
+// run 96-thread row groups (32 / VT rows each), one region per vector
+// (k_xprod_w) or seven per z row (k_xprod_m).
 int xprod_threads(int n, int rb)
 {
     if (!xprod_warp(n)) return fast_threads(n, 3 * rb);
@@ -902,13 +1133,15 @@ int xprod_threads(int n, int rb)
 
 size_t xprod_smem(int n, int rb)
 {
-    if (!xprod_warp(n)) return (size_t)n * ((3 * rb) | 1) * sizeof(double2);
+    const int mode = xprod_mode(n);
+    if (mode == 0) return (size_t)n * ((3 * rb) | 1) * sizeof(double2);
+    const int per_row = mode == 3 ? 7 : 3;
     switch (n) {
 #define LH_CASE(N)                                                                                  \
     case N: {                                                                                       \
         const int reg = N > Plan2<N>::N1 * (Plan2<N>::N2 + 1) ? N : Plan2<N>::N1 * (Plan2<N>::N2 + 1); \
         const int rg = 32 / fast_vector_threads(N);                                                 \
-        return (size_t)3 * rg * ((rb + rg - 1) / rg) * reg * sizeof(double2);                     \
+        return (size_t)per_row * rg * ((rb + rg - 1) / rg) * reg * sizeof(double2);               \
     }
         LH_FAST_SIZES(LH_CASE)
 #undef LH_CASE
@@ -985,6 +1218,7 @@ cudaError_t fast_set_attributes(int Mz, int Mx, size_t smz, size_t smx, size_t s
         e = raise_smem_limit((const void *)k_xprod_f<N>, smx); \
         if (e == cudaSuccess) e = raise_smem_limit((const void *)k_xprod_w<N, 0>, smx); \
         if (e == cudaSuccess) e = raise_smem_limit((const void *)k_xprod_w<N, 1>, smx); \
+        if (e == cudaSuccess) e = raise_smem_limit((const void *)k_xprod_m<N>, smx); \
         break;
         LH_FAST_SIZES(LH_CASE)
 #undef LH_CASE
@@ -1014,9 +1248,12 @@ void fast_launch_xprod(int Mx, unsigned grid, int threads, size_t smem, cudaStre
     switch (Mx) {
 #define LH_CASE(N)                                                                   \
     case N:                                                                          \
-        if (xprod_warp(N) && xprod_direct()) k_xprod_w<N, 1><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); \
-        else if (xprod_warp(N)) k_xprod_w<N, 0><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); \
-        else k_xprod_f<N><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); \
+        switch (xprod_mode(N)) {                                                     \
+        case 3: k_xprod_m<N><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); break; \
+        case 2: k_xprod_w<N, 1><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); break; \
+        case 1: k_xprod_w<N, 0><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); break; \
+        default: k_xprod_f<N><<<grid, threads, smem, st>>>(insts, work, count, rb, want_max); \
+        }                                                                            \
         break;
         LH_FAST_SIZES(LH_CASE)
 #undef LH_CASE

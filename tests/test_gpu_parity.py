@@ -352,6 +352,40 @@ def test_fast_and_generic_fft_paths_agree(N, monkeypatch):
         assert rel_l2(out[0][f], out[1][f]) <= (1e-12 if f == "p" else 1e-13), f
 
 
+@pytest.mark.parametrize("N,ny", [(32, 153), (32, 65), (32, 66), (128, 153)])
+def test_multi_plane_x_stage(N, ny, monkeypatch):
+    """The multi-plane x stage (LH_XPROD_WARP=3, where a vector fits a warp:
+    Mx = 48, 192) interpolates in y after the x transform instead of before
+    it, so it agrees with the default per-plane stage to round-off, CFL time
+    step included; and since its plane groups and v-row pairs sit at absolute
+    planes, another staging budget -- other rounds -- gives the same states
+    bit for bit.  ny = 153, 65 and 66 end on groups of 2, 4 and 5 planes (an
+    even last group pairs its top v row with the zero ghost)."""
+    from lh_b200 import Desc, grids, perturbed_laminar
+    d = Desc(Nx=N, Nz=N, ny=ny, dt_mode=0, CFL=0.5)
+    ic = perturbed_laminar(d, 17, *grids(d))
+    out = []
+    # a budget that still holds whole groups per round (32^2: 30 planes per
+    # round against 75; 128^2: 10 against 25)
+    mb = "8" if N == 32 else "48"
+    for env in ({"LH_XPROD_WARP": "3"}, {"LH_XPROD_WARP": "3", "LH_STAGING_MB": mb}, {}):
+        for k in ("LH_XPROD_WARP", "LH_STAGING_MB"):
+            if k in env:
+                monkeypatch.setenv(k, env[k])
+            else:
+                monkeypatch.delenv(k, raising=False)
+        e = _engine(d)
+        e.upload(*ic)
+        e.step(3)
+        e.synchronize()
+        out.append((e.download(), e.scalars()))
+    for f in FIELDS:
+        assert np.array_equal(out[0][0][f], out[1][0][f]), f
+        assert rel_l2(out[0][0][f], out[2][0][f]) <= (1e-12 if f == "p" else 1e-13), f
+    assert out[0][1] == out[1][1]
+    assert abs(out[0][1]["t"] - out[2][1]["t"]) <= 1e-13 * out[2][1]["t"]
+
+
 @pytest.mark.parametrize("N,ctpress,ny", [(16, 1, 97), (32, 0, 97), (64, 1, 97), (128, 1, 97), (32, 1, 257)])
 def test_small_and_sequential_column_passes_agree(N, ctpress, ny, monkeypatch):
     """The one-CTA-per-column pass (warp scans over the y rows) and the
