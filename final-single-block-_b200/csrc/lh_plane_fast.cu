@@ -49,6 +49,21 @@
 #ifndef LH_ZFWD_B
 #define LH_ZFWD_B 3
 #endif
+// The block-synchronous kernels at the largest length hold longer register
+// FFTs (24 threads per vector at Ngal 384): at three CTAs per SM (80
+// registers) they spilled 0.4-0.8 KB per thread.  From LH_LARGE_N on, the
+// bound is LH_LARGE_B CTAs per SM (128 registers, no spills).  Measured on
+// B200 (ms per RK3 step): 256^2 x 257 12.32 -> 10.15, the uneven batch
+// 4.92e9 -> 5.47e9 grid-pt*substeps/s; at Ngal 288 the kernels timed alone
+// gained but the step lost 1 % (the round streams overlap less), and at 192
+// both lost, so those sizes keep three CTAs.
+#ifndef LH_LARGE_N
+#define LH_LARGE_N 384
+#endif
+#ifndef LH_LARGE_B
+#define LH_LARGE_B 2
+#endif
+#define LH_MINB(N, B) ((N) >= LH_LARGE_N ? LH_LARGE_B : (B))
 // iterations of the warp-local x stage's gather loop unrolled (its loads of
 // later modes are then issued before the shared-memory stores of earlier ones)
 #ifndef LH_XGATHER_UNROLL
@@ -85,7 +100,7 @@ __device__ __forceinline__ double2 *sprod_slot(const Inst &I, int s)
 // z inverse of one (y row jp, field f in {u1, u3, u2}, block of cb x modes):
 // the pruned cft of four_to_phys_u (FOU3D.f90:653-679), -> Sin[slot][f]
 template <int NZ>
-__global__ void __launch_bounds__(LH_ZINV_T, LH_ZINV_B) k_zinv_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
+__global__ void __launch_bounds__(LH_ZINV_T, LH_MINB(NZ, LH_ZINV_B)) k_zinv_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
                                                          int count, int cb)
 {
     constexpr int N1 = Plan2<NZ>::N1, N2 = Plan2<NZ>::N2;
@@ -208,7 +223,7 @@ __global__ void __launch_bounds__(LH_ZINV_T, LH_ZINV_B) k_zinv_w(const Inst *__r
 // complex FFT), products, forward real x FFT (ops_in_planes2,
 // FOU3D.f90:1514-1652) -> Sprod[slot]
 template <int NX>
-__global__ void __launch_bounds__(LH_XPROD_T, LH_XPROD_B) k_xprod_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
+__global__ void __launch_bounds__(LH_XPROD_T, LH_MINB(NX, LH_XPROD_B)) k_xprod_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
                                                           int count, int rb, int want_max)
 {
     constexpr int N1 = Plan2<NX>::N1, N2 = Plan2<NX>::N2;
@@ -851,7 +866,7 @@ __global__ void __launch_bounds__(LH_XMULTI_T, LH_XMULTI_B) k_xprod_m(const Inst
 // halves: {uu, uw, ww} -> Nu1 and Nu3 x/z parts; {vv, uv, wv} -> vv_c, uv_f,
 // wv_f and the Nu2 x/z part.
 template <int NZ>
-__global__ void __launch_bounds__(LH_ZFWD_T, LH_ZFWD_B) k_zfwd_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
+__global__ void __launch_bounds__(LH_ZFWD_T, LH_MINB(NZ, LH_ZFWD_B)) k_zfwd_f(const Inst *__restrict__ insts, const Work *__restrict__ work,
                                                          int count, int cb)
 {
     constexpr int N1 = Plan2<NZ>::N1, N2 = Plan2<NZ>::N2;
