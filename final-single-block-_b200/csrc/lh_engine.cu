@@ -328,15 +328,18 @@ ClassTiles fast_tiles(const HostSetup &s, int cbz_max, int rb, int cbf_max)
 // Default tile bounds of a fast size: measured on B200 at 128^2 (16 threads
 // per vector): 16 x modes per z-inverse CTA, 4 z rows per x CTA, up to 4 x
 // modes per z-forward CTA; sizes with fewer threads per vector take
-// proportionally more.  The z-forward bound is 80/vz, one less at Mz = 96
+// proportionally more, the x stage at 18 and more one z row.  The z-forward bound is 80/vz, one less at Mz = 96
 // and 192 (ny = 153 sweeps: one x mode fewer was faster there, slower at
 // Mz = 288 and 384, even at 48).
 void default_bounds(const HostSetup &s, int &cbz, int &rbx, int &cbf)
 {
     const int vz = std::max(1, fast_vector_threads(s.Mz)), vx = std::max(1, fast_vector_threads(s.Mx));
     cbz = 256 / vz;
-    // the multi-plane x stage holds seven vectors per z row: one row group
-    rbx = std::max(1, (xprod_multi(s.Mx) ? 32 : 64) / vx);
+    // the multi-plane x stage holds seven vectors per z row: one row group;
+    // the block-synchronous stage at 18 and 24 threads per vector (Ngal 288,
+    // 384) is fastest with one z row per CTA (autotuner on B200: 192^2 x 257
+    // 5.43 -> 5.07 ms per step, 256^2 x 257 10.11 -> 9.76)
+    rbx = vx >= 18 && !xprod_warp(s.Mx) ? 1 : std::max(1, (xprod_multi(s.Mx) ? 32 : 64) / vx);
     cbf = std::max(1, 80 / vz - ((s.Mz == 96 || s.Mz == 192) ? 1 : 0));
 }
 

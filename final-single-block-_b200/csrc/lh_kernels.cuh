@@ -49,6 +49,7 @@ int fast_threads(int n, int vectors);
 int fast_max_threads(int stage);  // launch-bounds block size of a fast stage
 int fast_vector_threads(int n);   // threads per vector of a fast length
 size_t zinv_smem(int n, int cb);  // shared memory of a z-inverse CTA of cb vectors
+bool xprod_warp(int n);            // the x stage of length n runs a warp-local kernel
 bool xprod_multi(int n);           // the x stage of length n runs the multi-plane kernel
 int xprod_max_threads(int n);      // launch-bounds block size of that x-stage kernel
 int xprod_threads(int n, int rb);  // threads of an x-stage CTA of rb z rows
