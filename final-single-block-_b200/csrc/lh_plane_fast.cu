@@ -49,16 +49,15 @@
 #ifndef LH_ZFWD_B
 #define LH_ZFWD_B 3
 #endif
-// The block-synchronous kernels at the largest length hold longer register
-// FFTs (24 threads per vector at Ngal 384): at three CTAs per SM (80
-// registers) they spilled 0.4-0.8 KB per thread.  From LH_LARGE_N on, the
-// bound is LH_LARGE_B CTAs per SM (128 registers, no spills).  Measured on
-// B200 (ms per RK3 step): 256^2 x 257 12.32 -> 10.15, the uneven batch
-// 4.92e9 -> 5.47e9 grid-pt*substeps/s; at Ngal 288 the kernels timed alone
-// gained but the step lost 1 % (the round streams overlap less), and at 192
-// both lost, so those sizes keep three CTAs.
+// The block-synchronous kernels at the large lengths hold longer register
+// FFTs (18 and 24 threads per vector at Ngal 288 and 384): at three CTAs per
+// SM (80 registers) they spilled 0.1-0.8 KB per thread.  From LH_LARGE_N on,
+// the bound is LH_LARGE_B CTAs per SM (128 registers, no spills).  Measured
+// on B200 (ms per RK3 step): 256^2 x 257 12.32 -> 10.15; 192^2 x 257 5.04 ->
+// 4.88, x 153 3.11 -> 3.01, x 97 2.00 -> 1.93 (with one z row per x CTA; with
+// three it lost 1 %); at Ngal 192 two CTAs lost in the step graph.
 #ifndef LH_LARGE_N
-#define LH_LARGE_N 384
+#define LH_LARGE_N 288
 #endif
 #ifndef LH_LARGE_B
 #define LH_LARGE_B 2
