@@ -895,16 +895,33 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_column_small(const Inst *_
         double2 *N = (role == 0 ? I.NU1 : I.NU3) + col;
         const double dC3 = rk.d * (role == 0 ? kxr : kzr);
         const double C1m = (role == 0 && mean) ? -rk.d * I.sc[SC_MPGX] : 0.0;
-        for (int j = lane; j < R; j += 32) {
+        // rows in batches of kSmallBatch per lane, every global load of a batch
+        // issued before its arithmetic (the per-row operations are unchanged)
+        for (int jb = lane; jb < R; jb += 32 * kSmallBatch) {
+        double2 lno[kSmallBatch], lx[kSmallBatch], lfl[kSmallBatch], lflp[kSmallBatch];
+#pragma unroll
+        for (int b = 0; b < kSmallBatch; b++) {
+            const int j = jb + 32 * b;
+            lno[b] = lx[b] = lfl[b] = lflp[b] = z2;
+            if (j >= 1 && j <= nyu) {
+                const size_t o = (size_t)j * nc, on = o - nc;
+                // Nu_old is overwritten below by the same thread: a plain load
+                if (kRK != 1) lno[b] = SN[on];  // c_1 = 0: Nu_old unused at kRK = 1
+                lx[b] = __ldg(SX + on);
+                lfl[b] = __ldg(FL + o);
+                lflp[b] = __ldg(FL + on);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < kSmallBatch; b++) {
+            const int j = jb + 32 * b;
+            if (j >= R) break;
             if (j == 0 || j == nyu + 1) {
                 S[j] = make_double2(0.0, 0.0);
                 continue;
             }
             const double2 um = O[j - 1], uc = O[j], up = O[j + 1];
-            const size_t o = (size_t)j * nc, on = o - nc;
-            // Nu_old is overwritten below in this iteration: a plain load
-            const double2 no = kRK == 1 ? z2 : SN[on];  // c_1 = 0: Nu_old unused at kRK = 1
-            const double2 x = __ldg(SX + on), fl = __ldg(FL + o), flp = __ldg(FL + on);
+            const double2 no = lno[b], x = lx[b], fl = lfl[b], flp = lflp[b];
             const double2 pj = SP[j - 1];
             const double d1 = du[3 * j], d2 = du[3 * j + 1], d3 = du[3 * j + 2];
             const double cen = k2x + k2z + d2;
@@ -917,21 +934,37 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_column_small(const Inst *_
             dd = make_double2(dd.x + G * nu.x, dd.y + G * nu.y);
             S[j] = make_double2(uc.x + dt * dd.x, uc.y + dt * dd.y);
         }
+        }
         __syncwarp();
         small_solve(lane, nyu, du, beta, k2x, k2z, I.gw1, I.gw2, facu, invu, S);
     } else {
         double2 *N = I.NU2 + col;
         const double2 *SN2 = I.NU2 + col, *SX2 = I.NXZ2 + col, *SVV = I.VVC + col;
-        for (int j = lane; j < Rv; j += 32) {
+        for (int jb = lane; jb < Rv; jb += 32 * kSmallBatch) {
+        double2 lno[kSmallBatch], lx[kSmallBatch], lvc[kSmallBatch], lvn[kSmallBatch];
+#pragma unroll
+        for (int b = 0; b < kSmallBatch; b++) {
+            const int j = jb + 32 * b;
+            lno[b] = lx[b] = lvc[b] = lvn[b] = z2;
+            if (j >= 1 && j <= nyv) {
+                const size_t o = (size_t)j * nc, on = o - nc;
+                // Nu_old is overwritten below by the same thread: a plain load
+                if (kRK != 1) lno[b] = SN2[on];  // c_1 = 0: Nu_old unused at kRK = 1
+                lx[b] = __ldg(SX2 + on);
+                lvc[b] = __ldg(SVV + o);
+                lvn[b] = __ldg(SVV + o + nc);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < kSmallBatch; b++) {
+            const int j = jb + 32 * b;
+            if (j >= Rv) break;
             if (j == 0 || j == nyv + 1) {
                 S2[j] = make_double2(0.0, 0.0);
                 continue;
             }
             const double2 um = O2[j - 1], uc = O2[j], up = O2[j + 1];
-            const size_t o = (size_t)j * nc, on = o - nc;
-            // Nu_old is overwritten below in this iteration: a plain load
-            const double2 no = kRK == 1 ? z2 : SN2[on];  // c_1 = 0: Nu_old unused at kRK = 1
-            const double2 x = __ldg(SX2 + on), vvc = __ldg(SVV + o), vvn = __ldg(SVV + o + nc);
+            const double2 no = lno[b], x = lx[b], vvc = lvc[b], vvn = lvn[b];
             const double2 pc = SP[j - 1], pn = SP[j];
             const double e1 = dv[3 * j], e2 = dv[3 * j + 1], e3 = dv[3 * j + 2];
             const double cenv = k2x + k2z + e2;
@@ -943,6 +976,7 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_column_small(const Inst *_
             N[(size_t)(j - 1) * nc] = nu;
             dd = make_double2(dd.x + G * nu.x, dd.y + G * nu.y);
             S2[j] = make_double2(uc.x + dt * dd.x, uc.y + dt * dd.y);
+        }
         }
         __syncwarp();
         small_solve(lane, nyv, dv, beta, k2x, k2z, 0.0, 0.0, facv, invv, S2);

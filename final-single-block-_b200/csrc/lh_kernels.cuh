@@ -11,6 +11,8 @@ size_t column_smem_bytes(int max_nyu);  // ring + staged y metrics
 // column pass for small mode counts: one CTA of kSmallWarps warps (the u1,
 // u3, u2 chains) per column, rows spread over the lanes
 constexpr int kSmallWarps = 3;
+// rows per lane whose global loads the right-hand-side phase issues together
+constexpr int kSmallBatch = 4;
 size_t column_small_smem_bytes(int max_nyu);
 
 __global__ void k_zinv(const Inst *__restrict__ insts, const Work *__restrict__ work, int bc);
