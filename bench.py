@@ -229,7 +229,7 @@ def substep_alg_bytes(desc):
 # works on the L2-resident staging only, the z-forward writes the x/z parts
 # of Nu and the three y-flux spectra, the column pass reads 13 fields and
 # writes 7 (u1 u2 u3 p, Nu x3).
-DESIGN_F = {"z_inverse": 3, "x_products": 0, "z_forward": 6, "dt": 0, "column": 20}
+FIELD_PASSES = {"z_inverse": 3, "x_products": 0, "z_forward": 6, "dt": 0, "column": 20}
 
 
 def _batch_rate(b, pts, K):
@@ -403,7 +403,7 @@ def run_ours(args, rank, world, local_rank):
     kernels = {}
     for name, (kms, kn) in prof.items():
         per_sub = kms / 6.0  # 2 steps x 3 substeps
-        kb = DESIGN_F[name] * F
+        kb = FIELD_PASSES[name] * F
         kernels[name] = {"ms_per_substep": per_sub, "launches_per_substep": kn / 6.0,
                          "share": kms / sum(v[0] for v in prof.values()),
                          "design_hbm_bytes_per_substep": kb,
