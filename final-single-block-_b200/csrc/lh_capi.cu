@@ -77,8 +77,10 @@ extern "C" int lh_ctx_create(const lh_grid_desc *desc, lh_ctx **out)
 extern "C" int lh_ctx_destroy(lh_ctx *c)
 {
     if (!c) return LH_OK;
-    if (c->gexec) cudaGraphExecDestroy(c->gexec);
-    if (c->graph) cudaGraphDestroy(c->graph);
+    ctx_drop_graphs(c);
+    if (c->ev_u) cudaEventDestroy(c->ev_u);
+    if (c->ev_p) cudaEventDestroy(c->ev_p);
+    if (c->st_up) cudaStreamDestroy(c->st_up);
     plan_free(c->plan);
     if (c->d_inst) cudaFree(c->d_inst);
     if (c->d_spec) cudaFree(c->d_spec);
@@ -177,20 +179,31 @@ extern "C" int lh_substep(lh_ctx *c, int kRK)
     return LH_OK;
 }
 
-static int ensure_graph(lh_ctx *c)
+// Capture one RK3 step; with wait_p (lh_step_host's first step) the first
+// column pass waits for ev_p, the end of the p upload.
+static int capture_step(lh_ctx *c, cudaEvent_t wait_p, cudaGraph_t *graph, cudaGraphExec_t *gexec)
 {
-    if (c->gexec) return LH_OK;
     CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal), "graph capture");
     cudaError_t el = cudaSuccess;
     for (int k = 1; k <= 3 && el == cudaSuccess; k++)
-        el = launch_substep(c->plan, c->d_inst, k, c->dev.desc.dt_mode == LH_DT_CFL, c->st);
+        el = launch_substep(c->plan, c->d_inst, k, c->dev.desc.dt_mode == LH_DT_CFL, c->st, nullptr,
+                            k == 1 ? wait_p : nullptr);
     cudaGraph_t g = nullptr;
     cudaError_t ee = cudaStreamEndCapture(c->st, &g);
-    if (el != cudaSuccess) return cuda_fail(c, el, "graph capture launch");
+    if (el != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_fail(c, el, "graph capture launch");
+    }
     if (ee != cudaSuccess) return cuda_fail(c, ee, "graph capture end");
-    c->graph = g;
-    CK(cudaGraphInstantiate(&c->gexec, g, 0), "graph instantiate");
+    *graph = g;
+    CK(cudaGraphInstantiate(gexec, g, 0), "graph instantiate");
     return LH_OK;
+}
+
+static int ensure_graph(lh_ctx *c)
+{
+    if (c->gexec) return LH_OK;
+    return capture_step(c, nullptr, &c->graph, &c->gexec);
 }
 
 extern "C" int lh_step(lh_ctx *c, int nsteps)
@@ -204,12 +217,41 @@ extern "C" int lh_step(lh_ctx *c, int nsteps)
     return LH_OK;
 }
 
+// Upload, nsteps steps, download.  u1, u2 and u3 upload first on st_up; p
+// follows on st_up while the first substep's plane pass (which does not read
+// p) runs on st, and the first column pass waits for it; the PCIe transfer
+// of p is then hidden behind the plane pass.  Same operations and results as
+// lh_upload_state + lh_step + lh_download_state.
 extern "C" int lh_step_host(lh_ctx *c, double *u1, double *u2, double *u3, double *p, int nsteps)
 {
-    int rc = lh_upload_state(c, u1, u2, u3, p);
-    if (rc) return rc;
-    if ((rc = lh_step(c, nsteps))) return rc;
-    if ((rc = lh_download_state(c, u1, u2, u3, p))) return rc;
+    if (!c || !u1 || !u2 || !u3) return fail(c, LH_EINVAL, "u1, u2 and u3 are required");
+    if (nsteps < 0) return fail(c, LH_EINVAL, "nsteps < 0");
+    if (!c->st_up) {
+        CK(cudaStreamCreateWithFlags(&c->st_up, cudaStreamNonBlocking), "upload stream");
+        CK(cudaEventCreateWithFlags(&c->ev_u, cudaEventDisableTiming), "upload event");
+        CK(cudaEventCreateWithFlags(&c->ev_p, cudaEventDisableTiming), "upload event");
+    }
+    // the upload reuses the staging field the previous call's download used
+    CK(cudaStreamSynchronize(c->st), "synchronize");
+    CK(instance_upload_p_last(c->dev, u1, u2, u3, p, c->st_up, c->ev_u), "upload");
+    CK(cudaEventRecord(c->ev_p, c->st_up), "upload");
+    c->have_state = true;
+    CK(cudaStreamWaitEvent(c->st, c->ev_u, 0), "upload wait");
+    if (nsteps == 0) {
+        CK(cudaStreamWaitEvent(c->st, c->ev_p, 0), "upload wait");
+    } else {
+        int rc = LH_OK;
+        if (!c->gexec_host) rc = capture_step(c, c->ev_p, &c->graph_host, &c->gexec_host);
+        if (rc == LH_OK) rc = ensure_graph(c);
+        if (rc) {
+            cudaStreamSynchronize(c->st_up);
+            return rc;
+        }
+        CK(cudaGraphLaunch(c->gexec_host, c->st), "graph launch");
+        for (int s = 1; s < nsteps; s++) CK(cudaGraphLaunch(c->gexec, c->st), "graph launch");
+    }
+    CK(instance_download(c->dev, u1, u2, u3, p, c->st), "download");
+    CK(cudaStreamSynchronize(c->st_up), "synchronize");
     return check_err_word(c);
 }
 

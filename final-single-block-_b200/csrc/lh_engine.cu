@@ -234,8 +234,9 @@ cudaError_t download_field(const DevInstance &d, const double2 *src, int len, do
     return cudaMemcpyAsync(dst, d.stage, (size_t)len * nc * sizeof(double2), cudaMemcpyDeviceToHost, st);
 }
 
-cudaError_t instance_upload(DevInstance &d, const double *u1, const double *u2, const double *u3, const double *p,
-                            cudaStream_t st)
+// The fields but p, the Nu reset and the scalars of an upload (getini).
+static cudaError_t upload_without_p(DevInstance &d, const double *u1, const double *u2, const double *u3,
+                                    cudaStream_t st)
 {
     const HostSetup &s = d.hs;
     Inst &I = d.inst;
@@ -243,7 +244,6 @@ cudaError_t instance_upload(DevInstance &d, const double *u1, const double *u2, 
     if ((e = upload_field(d, u1, I.U1, s.nyu + 2, st)) != cudaSuccess) return e;
     if ((e = upload_field(d, u2, I.U2, s.nyv + 2, st)) != cudaSuccess) return e;
     if ((e = upload_field(d, u3, I.U3, s.nyu + 2, st)) != cudaSuccess) return e;
-    if ((e = upload_field(d, p, I.P, s.nyu, st)) != cudaSuccess) return e;
     const size_t npc = (size_t)s.nyu * s.nc * sizeof(double2);
     // Nu = 0 before the first step (littleharsh.f90:127-129)
     if ((e = cudaMemsetAsync(I.NU1, 0, npc, st)) != cudaSuccess) return e;
@@ -257,8 +257,25 @@ cudaError_t instance_upload(DevInstance &d, const double *u1, const double *u2, 
     sc[SC_QX] = q;
     sc[SC_QXT] = q;  // getini: QxT = Qx for the constant flow-rate mode
     if ((e = cudaMemcpyAsync(I.sc, sc, sizeof(sc), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(I.err, 0, sizeof(int), st)) != cudaSuccess) return e;
+    return cudaMemsetAsync(I.err, 0, sizeof(int), st);
+}
+
+cudaError_t instance_upload(DevInstance &d, const double *u1, const double *u2, const double *u3, const double *p,
+                            cudaStream_t st)
+{
+    cudaError_t e = upload_without_p(d, u1, u2, u3, st);
+    if (e == cudaSuccess) e = upload_field(d, p, d.inst.P, d.hs.nyu, st);
+    if (e != cudaSuccess) return e;
     return cudaStreamSynchronize(st);
+}
+
+cudaError_t instance_upload_p_last(DevInstance &d, const double *u1, const double *u2, const double *u3,
+                                   const double *p, cudaStream_t st, cudaEvent_t ev_u)
+{
+    cudaError_t e = upload_without_p(d, u1, u2, u3, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev_u, st);
+    if (e == cudaSuccess) e = upload_field(d, p, d.inst.P, d.hs.nyu, st);
+    return e;
 }
 
 cudaError_t instance_download(DevInstance &d, double *u1, double *u2, double *u3, double *p, cudaStream_t st)
@@ -663,7 +680,7 @@ static cudaError_t time_end(LaunchTimer *t, int cls, cudaStream_t st)
 }
 
 cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl_any, cudaStream_t st,
-                           LaunchTimer *timer)
+                           LaunchTimer *timer, cudaEvent_t before_column)
 {
     const int want_max = (kRK == 1 && cfl_any) ? 1 : 0;
     cudaError_t e = cudaSuccess;
@@ -735,6 +752,7 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
         k_dt<<<p.ninst, 256, 0, st>>>(d_insts, p.ninst);
         if ((e = time_end(timer, 3, st)) != cudaSuccess) return e;
     }
+    if (before_column && (e = cudaStreamWaitEvent(st, before_column, cudaEventWaitExternal)) != cudaSuccess) return e;
     time_begin(timer, st);
     if (p.col_split) {
         if (!a_beside)

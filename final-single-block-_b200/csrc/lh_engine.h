@@ -50,6 +50,11 @@ void instance_free(DevInstance &d);
 // Upload / download the four state fields in the reference column layout.
 cudaError_t instance_upload(DevInstance &d, const double *u1, const double *u2, const double *u3, const double *p,
                             cudaStream_t st);
+// The same upload with p last: everything the plane pass and the column pass
+// read except p is enqueued on st, then ev_u is recorded on st, then p is
+// enqueued; nothing waits on the host.
+cudaError_t instance_upload_p_last(DevInstance &d, const double *u1, const double *u2, const double *u3,
+                                   const double *p, cudaStream_t st, cudaEvent_t ev_u);
 cudaError_t instance_download(DevInstance &d, double *u1, double *u2, double *u3, double *p, cudaStream_t st);
 cudaError_t download_field(const DevInstance &d, const double2 *src, int len, double *dst, cudaStream_t st);
 
@@ -144,8 +149,10 @@ void tune_store(int Mz, int Mx, int nyu, const TuneParams &t);
 cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, bool force_generic = false,
                        const TuneParams *force = nullptr);
 void plan_free(Plan &p);
-// Enqueue one substep of every instance of the plan.
+// Enqueue one substep of every instance of the plan.  With before_column the
+// column pass first waits for that event (an external event node when
+// captured): the plane pass does not read p, so p may still be uploading.
 cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl_any, cudaStream_t st,
-                           LaunchTimer *timer = nullptr);
+                           LaunchTimer *timer = nullptr, cudaEvent_t before_column = nullptr);
 
 }  // namespace lh

@@ -230,10 +230,7 @@ extern "C" int lh_autotune(lh_ctx *c, int force, int *params)
     tune_store(s.Mz, s.Mx, s.nyu, best);
     // the context's own plan picks the tuned parameters up; its step graph is
     // captured again on the next lh_step
-    if (c->gexec) cudaGraphExecDestroy(c->gexec);
-    if (c->graph) cudaGraphDestroy(c->graph);
-    c->gexec = nullptr;
-    c->graph = nullptr;
+    ctx_drop_graphs(c);
     const char *gen = getenv("LH_GENERIC_FFT");
     cudaError_t e = plan_build(c->plan, {&c->dev}, gen && gen[0] == '1');
     if (e != cudaSuccess) {

@@ -327,6 +327,24 @@ def test_step_host_matches_device_path():
     e2.step_host(bufs, 2)
     for f, b in zip(FIELDS, bufs):
         assert np.array_equal(b, ref[f]), f
+    # p uploads beside the first plane pass: no steps is an exact round trip,
+    # and repeated one-step calls (each a fresh upload) equal the device path
+    e3 = _engine(d)
+    bufs = [np.ascontiguousarray(x).copy() for x in ic]
+    e3.step_host(bufs, 0)
+    for x, b in zip(ic, bufs):
+        assert np.array_equal(b, np.ascontiguousarray(x))
+    want = [np.ascontiguousarray(x).copy() for x in ic]
+    for _ in range(2):
+        e4 = _engine(d)
+        e4.upload(*want)
+        e4.step(1)
+        e4.synchronize()
+        r = e4.download()
+        want = [r[f] for f in FIELDS]
+        e3.step_host(bufs, 1)
+    for f, w, b in zip(FIELDS, want, bufs):
+        assert np.array_equal(b, w), f
 
 
 @pytest.mark.parametrize("N", [32, 64, 128, 192, 256])
