@@ -103,7 +103,9 @@ int lh_step(lh_ctx *ctx, int nsteps);
 int lh_get_scalars(lh_ctx *ctx, double *t, double *dt, int *iter,
                    double *mpgx, double *Qx);
 /* Host-buffer step for callers that keep the state on the host: upload,
- * nsteps RK3 steps, download (the Fortran drop-in call). */
+ * nsteps RK3 steps, download (the Fortran drop-in call).  Same results as
+ * lh_upload_state + lh_step + lh_download_state; p is uploaded beside the
+ * first substep's plane pass.  Synchronous: returns after the download. */
 int lh_step_host(lh_ctx *ctx, double *u1, double *u2, double *u3, double *p,
                  int nsteps);
 int lh_synchronize(lh_ctx *ctx);
