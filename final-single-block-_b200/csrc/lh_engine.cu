@@ -684,6 +684,12 @@ cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl
 {
     const int want_max = (kRK == 1 && cfl_any) ? 1 : 0;
     cudaError_t e = cudaSuccess;
+    // a split column pass reads p in the forward-sweep chunks beside the
+    // plane rounds: there the whole substep waits for before_column
+    if (before_column && p.col_split) {
+        if ((e = cudaStreamWaitEvent(st, before_column, cudaEventWaitExternal)) != cudaSuccess) return e;
+        before_column = nullptr;
+    }
     // round r on stream r % kRoundStreams (0 = st; their staging shares are
     // disjoint), forked from st after the work the plane pass depends on and
     // joined back before the work that consumes it; timed profiles keep one

@@ -151,7 +151,8 @@ cudaError_t plan_build(Plan &p, const std::vector<const DevInstance *> &insts, b
 void plan_free(Plan &p);
 // Enqueue one substep of every instance of the plan.  With before_column the
 // column pass first waits for that event (an external event node when
-// captured): the plane pass does not read p, so p may still be uploading.
+// captured): the plane pass does not read p, so p may still be uploading
+// (with a split column pass, whose chunks read p, the substep waits first).
 cudaError_t launch_substep(const Plan &p, const Inst *d_insts, int kRK, bool cfl_any, cudaStream_t st,
                            LaunchTimer *timer = nullptr, cudaEvent_t before_column = nullptr);
 

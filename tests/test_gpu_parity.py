@@ -347,6 +347,25 @@ def test_step_host_matches_device_path():
         assert np.array_equal(b, w), f
 
 
+def test_step_host_with_split_column_pass(monkeypatch):
+    """With the column pass split into chunks beside the plane rounds (they
+    read p), the host-buffer step still equals upload + step + download."""
+    from lh_b200 import Desc, grids, perturbed_laminar
+    monkeypatch.setenv("LH_SMALL_COLUMNS", "0")
+    monkeypatch.setenv("LH_COLUMN_SPLIT", "1")
+    d = Desc(Nx=64, Nz=64, ny=97, dt_mode=1, dt=5e-4)
+    ic = perturbed_laminar(d, 21, *grids(d))
+    e = _engine(d)
+    e.upload(*ic)
+    e.step(2)
+    e.synchronize()
+    ref = e.download()
+    bufs = [np.ascontiguousarray(x).copy() for x in ic]
+    _engine(d).step_host(bufs, 2)
+    for f, b in zip(FIELDS, bufs):
+        assert np.array_equal(b, ref[f]), f
+
+
 @pytest.mark.parametrize("N", [32, 64, 128, 192, 256])
 def test_fast_and_generic_fft_paths_agree(N, monkeypatch):
     """The compile-time-sized plane kernels and the generic ones give the
